@@ -1,0 +1,295 @@
+"""Benchmark of the distance-driven projector pair on B200.
+
+Workload (one step): forward projection A x followed by backprojection A^T b of
+one 2048 x 2048 float32 slice at 1800 angles uniform on [0, 180), 2048 detector
+bins, seeded random-ellipse phantom (synthetic data).  Metric: GUPS, i.e.
+pixel x angle updates per second (2 * 2048^2 * 1800 updates per step), higher
+is better.  Between timed steps L2 is flushed by writing a 256 MiB buffer.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 runs under torchrun, one rank per GPU, each rank projecting its own
+slices (independent slices: weak scaling, no collective on the data path);
+the step time is the max over ranks.  ``--impl reference`` times the
+reference's own C kernel (compiled into oracle/_ref) on the host cores, on a
+bounded sample of angles of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+N_SIDE, N_ANG = 2048, 1800
+METRIC = "dd projector pair GUPS (pixel x angle updates per second, forward + adjoint)"
+UNIT = "GUPS"
+WORKLOAD = "distance-driven pair, 2048x2048 image, 1800 angles [0,180), 2048 bins, float32"
+TAU_DD = 2  # gathered operand values per update (distance-driven)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-sample-angles", type=int, default=0,
+                    help="angles per step of the CPU baseline sample (0: auto)")
+    return ap.parse_args()
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.lines = []
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in getattr(self, "lines", []):
+            f = [x.strip() for x in l.split(",")]
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except (ValueError, IndexError):
+                continue
+            for nm, val in zip(names, f[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_reference_gups(n: int, na_total: int, sample_angles: int, threads: int):
+    """Reference dd kernel (oracle/_ref/ref_dd.so) on a sample of the angles.
+
+    Returns (GUPS, seconds, description).  ``threads`` > 1 runs that many
+    angle chunks concurrently (ctypes releases the GIL during the C call).
+    """
+    from concurrent.futures import ThreadPoolExecutor
+
+    from oracle.oracle import RefLib, radon_angles
+    from iterative_tomographic_reconstruction_algorithms_b200.phantom import angles_deg, random_ellipses
+    R = RefLib()
+    ang_all = radon_angles(angles_deg(na_total))
+    idx = np.linspace(0, na_total - 1, sample_angles).astype(int)
+    ang = np.ascontiguousarray(np.fft.fftshift(ang_all)[idx])
+    img = random_ellipses(n, seed=0)
+    chunks = np.array_split(np.arange(len(ang)), threads)
+    import ctypes
+    fp = ctypes.POINTER(ctypes.c_float)
+
+    def run(ch, oper):
+        a = np.ascontiguousarray(ang[ch])
+        if oper == 0:
+            out = np.zeros((len(a), n), np.float32)
+            R.L["dd"].radon_dd(img.ctypes.data_as(fp), n, a.ctypes.data_as(fp), len(a), 0,
+                               out.ctypes.data_as(fp))
+        else:
+            s = np.ones((len(a), n), np.float32)
+            out = np.zeros((n, n), np.float32)
+            R.L["dd"].radon_dd(out.ctypes.data_as(fp), n, a.ctypes.data_as(fp), len(a), 1,
+                               s.ctypes.data_as(fp))
+        return out
+
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(max_workers=threads) as ex:
+        list(ex.map(lambda c: run(c, 0), chunks))
+        list(ex.map(lambda c: run(c, 1), chunks))
+    dt = time.perf_counter() - t0
+    updates = 2.0 * n * n * len(ang)
+    desc = (f"reference radon_dd (oracle/_ref, -O3 -ffast-math) forward+adjoint on {len(ang)} of "
+            f"{na_total} angles at {n}x{n}, {threads} thread(s)")
+    return updates / dt / 1e9, dt, desc
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    sample = args.cpu_sample_angles or max(threads, 8)
+    vals = []
+    for i in range(args.warmup + args.steps):
+        g, dt, desc = cpu_reference_gups(N_SIDE, N_ANG, sample, threads)
+        if i >= args.warmup:
+            vals.append((g, dt))
+    gups = float(np.median([v[0] for v in vals]))
+    ms = float(np.median([v[1] for v in vals])) * 1e3
+    line = {"impl": "reference", "metric": METRIC, "value": gups, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "sample": desc},
+            "cpu_baseline": {"value": gups, "unit": UNIT, "cores": threads, "kind": "reference",
+                             "sample": desc},
+            "e2e": {"value": gups, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import torch
+    import torch.distributed as dist
+    from iterative_tomographic_reconstruction_algorithms_b200 import _lib
+    from iterative_tomographic_reconstruction_algorithms_b200 import class_projectors_radon as cpr
+    from iterative_tomographic_reconstruction_algorithms_b200.phantom import angles_deg, random_ellipses
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+
+    n, na = N_SIDE, N_ANG
+    deg = angles_deg(na)
+    tp = cpr.projectors(n, deg, oper="dd")
+    img_np = random_ellipses(n, seed=1000 + rank)
+    x = torch.from_numpy(img_np).to(dev)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MiB > L2
+    stream = torch.cuda.current_stream(dev)
+
+    import ctypes
+    s_gbs, l1_gbs, f_tf = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+    _lib.lib.tomo_measure_onchip_peaks.argtypes = [ctypes.POINTER(ctypes.c_double)] * 3
+    _lib.check(_lib.lib.tomo_measure_onchip_peaks(ctypes.byref(s_gbs), ctypes.byref(l1_gbs),
+                                                   ctypes.byref(f_tf)), "onchip peaks")
+
+    def step(events=None):
+        flush.fill_(1.0)
+        if events is not None:
+            events[0].record(stream)
+        b = tp.A(x)
+        if events is not None:
+            events[1].record(stream)
+        y = tp.At(b)
+        if events is not None:
+            events[2].record(stream)
+        return b, y
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        t0.record(stream)
+        for k in range(args.steps):
+            step(evs[k])
+        t1.record(stream)
+        torch.cuda.synchronize()
+    total_ms = t0.elapsed_time(t1)
+    fwd_ms = float(np.mean([e[0].elapsed_time(e[1]) for e in evs]))
+    adj_ms = float(np.mean([e[1].elapsed_time(e[2]) for e in evs]))
+    if world > 1:
+        t = torch.tensor([total_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    ms_step = total_ms / args.steps
+    updates_step = 2.0 * n * n * na  # per rank
+    value = updates_step * world / (ms_step * 1e-3) / 1e9
+
+    # end to end through the public API with host arrays (numpy in, numpy out)
+    b_np = tp.A(img_np)
+    torch.cuda.synchronize()
+    e2e_steps = max(2, min(args.steps, 5))
+    for _ in range(1):
+        tp.At(tp.A(img_np))
+    t_e = time.perf_counter()
+    for _ in range(e2e_steps):
+        b_np = tp.A(img_np)
+        g_np = tp.At(b_np)
+    e2e_s = (time.perf_counter() - t_e) / e2e_steps
+    e2e_val = updates_step * world / e2e_s / 1e9
+    h2d = img_np.nbytes + b_np.nbytes
+    d2h = b_np.nbytes + g_np.nbytes
+
+    # roofline of the dominant kernel (per survey: L1/shared-memory gather bound)
+    dom_ms = max(fwd_ms, adj_ms)
+    dom = "adjoint" if adj_ms >= fwd_ms else "forward"
+    upd_app = n * n * na
+    alg_bytes = 4.0 * TAU_DD * upd_app
+    achieved = alg_bytes / (dom_ms * 1e-3) / 1e9
+    peak = l1_gbs.value
+    roofline = {"bound": "l1", "kernel": f"dd_{dom}", "achieved": achieved, "peak": peak,
+                "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                "peak_source": "tomo_measure_onchip_peaks (4-byte L1 loads, this run)"}
+    hbm_bytes = 4.0 * (n * n + na * n)
+    peaks_file = ROOT / "MEASURED_PEAKS.json"
+    hbm_peak = json.loads(peaks_file.read_text())["hbm_gbs"] if peaks_file.exists() else 6650.0
+
+    if rank == 0:
+        cpu = None
+        if world == 1:
+            g, dt, desc = cpu_reference_gups(n, na, 4, 1)
+            cpu = {"value": g, "unit": UNIT, "cores": 1, "kind": "reference", "sample": desc}
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "slices_per_rank_per_step": 1,
+                       "l2": "flushed between steps (256 MiB write)", "parallelism": f"slices x{world}"},
+            "gpu_launches": 3 * args.steps,
+            "kernel_ms": {"dd_forward(+transpose)": fwd_ms, "dd_adjoint": adj_ms},
+            "roofline": roofline,
+            "roofline_hbm": {"bound": "hbm", "achieved": hbm_bytes / (dom_ms * 1e-3) / 1e9,
+                             "peak": hbm_peak, "unit": "GB/s",
+                             "frac": hbm_bytes / (dom_ms * 1e-3) / 1e9 / hbm_peak},
+            "onchip_peaks": {"smem_gbs": s_gbs.value, "l1_gbs": l1_gbs.value, "fp32_tflops": f_tf.value},
+            "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h)},
+            "clocks": clk.summary(),
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,114 @@
+/*
+ * tomo_b200.h -- C ABI of libtomo_b200.so, the B200 (sm_100a) projector pair
+ * behind the reference's projector classes.
+ *
+ * Two layers:
+ *
+ * 1. Drop-in entry points (tomo_radon_*, tomo_gen_*, tomo_gridrec_*).  Each one
+ *    has the argument list and meaning of one reference C function, so that a
+ *    binding which used to call the reference C can call this instead.  Host
+ *    pointers, synchronous, and -- like the reference C -- they ACCUMULATE into
+ *    the output array (the reference's Cython shims always pass zeros).
+ *    Differences: every function returns an int status instead of void (0 on
+ *    success, see TOMO_E*), and inputs the reference C would read or write out
+ *    of bounds are rejected with TOMO_EINVAL instead.
+ *
+ * 2. Plan API (tomo_plan_*, tomo_forward, tomo_adjoint, solver steps).  Device
+ *    pointers and a caller stream (cudaStream_t passed as void*), stream-ordered,
+ *    no allocation per call, a batch of nz slices per call.  Outputs are
+ *    overwritten.  The *_host variants take host pointers and do the copies.
+ *
+ * Conventions shared by both layers (they are the reference's):
+ *   image    float32 [n][n] row-major (C order), n = npix;
+ *   sinogram float32 [na][n], one row per angle;
+ *   angles   exactly the array the reference C function receives, i.e. AFTER
+ *            its Cython shim: radians for pd/rd/dd/ss (fftshifted for pd and
+ *            dd), degrees for the B-spline and gridding pairs.
+ * Sine and cosine of every angle are evaluated on the host with the C
+ * library's sincosf(), as the compiled reference does.
+ *
+ * Thread safety: a plan may be used from one host thread at a time; distinct
+ * plans are independent.  The drop-in entry points serialise internally.
+ */
+#ifndef TOMO_B200_H
+#define TOMO_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---- */
+#define TOMO_OK 0
+#define TOMO_ENOMEM 12      /* device or pinned-host allocation failed */
+#define TOMO_EINVAL 22      /* bad shape, kind, angle or parameter */
+#define TOMO_ETIMEDOUT 110  /* a bounded device wait gave up */
+#define TOMO_ECUDA 1000     /* CUDA runtime error; message via tomo_last_error */
+
+/* ---- projector kinds ---- */
+#define TOMO_KIND_PD 0      /* pixel-driven, linear (radon_pd.c method 1) */
+#define TOMO_KIND_RD 1      /* ray-driven / Siddon (radon_rd.c) */
+#define TOMO_KIND_DD 2      /* distance-driven (radon_dd.c) */
+#define TOMO_KIND_SS 3      /* slant-stacking, linear (radon_ss.c method 1) */
+#define TOMO_KIND_BSPLINE 4 /* generalised Radon of B-splines (gen_forwproj.c) */
+#define TOMO_KIND_GRID 5    /* gridding / Fourier slice (gridrec_v4_*.c) */
+
+typedef struct tomo_plan tomo_plan;
+
+typedef struct tomo_geom {
+  int kind;             /* TOMO_KIND_* */
+  int n;                /* image side = detector bins (reference: sino(nang, npix)) */
+  int na;               /* number of angles */
+  int nz;               /* slices per call (>= 1); arrays are [nz][...] */
+  const float *angles;  /* host, na entries, see conventions above */
+  /* B-spline pair (gen_forwproj.c:22-25): LUT [na][lut_size] and its support */
+  const float *lut;
+  int lut_size;
+  float support;
+  /* gridding pair (gridrec_v4.pyx:28-86): param[8], lut[len], deapod[pdim*pdim] */
+  const float *grid_param;
+  const float *grid_lut;
+  int grid_lut_len;
+  const float *grid_deapod;
+  int grid_mode;        /* 0 = compat (reference arithmetic), 1 = matched adjoint */
+} tomo_geom;
+
+/* Last error message of the calling thread ("" if none).  Returns TOMO_OK. */
+int tomo_last_error(char *buf, size_t len);
+
+/* Library version string, e.g. "tomo_b200 0.1 sm_100a". */
+const char *tomo_version(void);
+
+/* Measures, on the current device and at its current clocks, the shared-memory
+ * load bandwidth (16-byte conflict-free loads), the L1 load bandwidth (4-byte
+ * loads that hit L1) and the FP32 FMA rate.  These are the roofline
+ * denominators of the projector kernels (gather- and issue-bound, not HBM).
+ * No reference counterpart. */
+int tomo_measure_onchip_peaks(double *smem_gbs, double *l1_gbs, double *fp32_tflops);
+
+/* ---- plan API ---- */
+int tomo_plan_create(const tomo_geom *geom, tomo_plan **plan);
+int tomo_plan_destroy(tomo_plan *plan);
+
+/* Forward A: d_image [nz][n][n] -> d_sino [nz][na][n] (overwritten). */
+int tomo_forward(tomo_plan *plan, const float *d_image, float *d_sino, void *stream);
+/* Adjoint A^T: d_sino [nz][na][n] -> d_image [nz][n][n] (overwritten). */
+int tomo_adjoint(tomo_plan *plan, const float *d_sino, float *d_image, void *stream);
+/* Same, host arrays in and out (copies through pinned staging; synchronous). */
+int tomo_forward_host(tomo_plan *plan, const float *h_image, float *h_sino);
+int tomo_adjoint_host(tomo_plan *plan, const float *h_sino, float *h_image);
+
+/* ---- drop-in entry points (reference C signatures; host pointers) ---- */
+
+/* radon_dd.c:54 `void radon_dd(float* image, int npix, float* angles, int nang,
+ * int oper, float* sino)`, bound at radon_distance_driven.pyx:7.  Angles must
+ * lie in [-pi/2, pi] (outside it the reference's boundary merge is undefined). */
+int tomo_radon_dd(float *image, int npix, const float *angles, int nang, int oper,
+                  float *sino);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TOMO_B200_H */

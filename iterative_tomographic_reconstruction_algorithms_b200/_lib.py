@@ -1,0 +1,177 @@
+"""ctypes binding of libtomo_b200.so (include/tomo_b200.h).
+
+The shared library is built in-tree (``csrc/Makefile``) and is the only
+compute path: there is no CPU fallback.  Importing this module on a machine
+without the library raises immediately; calling a projector on a machine
+without a CUDA device raises at plan creation.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+from pathlib import Path
+
+import numpy as np
+
+PKG_DIR = Path(__file__).resolve().parent
+LIB_PATH = PKG_DIR / "libtomo_b200.so"
+
+TOMO_OK = 0
+TOMO_ENOMEM = 12
+TOMO_EINVAL = 22
+TOMO_ETIMEDOUT = 110
+TOMO_ECUDA = 1000
+
+KIND_PD, KIND_RD, KIND_DD, KIND_SS, KIND_BSPLINE, KIND_GRID = range(6)
+KIND_NAMES = {"pd": KIND_PD, "rd": KIND_RD, "dd": KIND_DD, "ss": KIND_SS,
+              "bspline": KIND_BSPLINE, "grid": KIND_GRID}
+
+_f32p = ctypes.POINTER(ctypes.c_float)
+
+
+class TomoGeom(ctypes.Structure):
+    _fields_ = [
+        ("kind", ctypes.c_int),
+        ("n", ctypes.c_int),
+        ("na", ctypes.c_int),
+        ("nz", ctypes.c_int),
+        ("angles", _f32p),
+        ("lut", _f32p),
+        ("lut_size", ctypes.c_int),
+        ("support", ctypes.c_float),
+        ("grid_param", _f32p),
+        ("grid_lut", _f32p),
+        ("grid_lut_len", ctypes.c_int),
+        ("grid_deapod", _f32p),
+        ("grid_mode", ctypes.c_int),
+    ]
+
+
+class TomoError(RuntimeError):
+    """A libtomo_b200 call returned a non-zero status."""
+
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+def _load() -> ctypes.CDLL:
+    if not LIB_PATH.exists():
+        raise ImportError(
+            f"{LIB_PATH} is missing: build it with `make -C {PKG_DIR / 'csrc'}` "
+            "(or __graft_entry__.build()); there is no CPU fallback")
+    lib = ctypes.CDLL(str(LIB_PATH), mode=os.RTLD_GLOBAL)
+    vp, i, f = ctypes.c_void_p, ctypes.c_int, ctypes.c_float
+    lib.tomo_last_error.argtypes = [ctypes.c_char_p, ctypes.c_size_t]
+    lib.tomo_version.restype = ctypes.c_char_p
+    lib.tomo_plan_create.argtypes = [ctypes.POINTER(TomoGeom), ctypes.POINTER(vp)]
+    lib.tomo_plan_destroy.argtypes = [vp]
+    for name in ("tomo_forward", "tomo_adjoint"):
+        getattr(lib, name).argtypes = [vp, vp, vp, vp]
+    for name in ("tomo_forward_host", "tomo_adjoint_host"):
+        getattr(lib, name).argtypes = [vp, vp, vp]
+    lib.tomo_radon_dd.argtypes = [_f32p, i, _f32p, i, i, _f32p]
+    return lib
+
+
+lib = _load()
+
+
+def last_error() -> str:
+    buf = ctypes.create_string_buffer(1024)
+    lib.tomo_last_error(buf, len(buf))
+    return buf.value.decode(errors="replace")
+
+
+def check(rc: int, what: str = "") -> None:
+    if rc != TOMO_OK:
+        msg = last_error()
+        if rc == TOMO_EINVAL:
+            raise ValueError(f"{what}: {msg}")
+        raise TomoError(rc, f"{what}: {msg}")
+
+
+def _torch():
+    import torch  # deferred: numpy-only users never pay the import
+    return torch
+
+
+class Plan:
+    """One projector geometry on one device (a ``tomo_plan``).
+
+    ``angles_c`` is the angle array exactly as the reference C function
+    receives it (after its Cython shim).  ``forward``/``adjoint`` accept either
+    numpy arrays (host path: copies in and out, returns numpy) or CUDA float32
+    torch tensors (device path on the current stream, returns a tensor).
+    """
+
+    def __init__(self, kind: int, n: int, angles_c: np.ndarray, nz: int = 1, **extra):
+        self.kind, self.n, self.nz = int(kind), int(n), int(nz)
+        self.angles_c = np.ascontiguousarray(angles_c, dtype=np.float32)
+        self.na = len(self.angles_c)
+        self._keep = [self.angles_c]
+        g = TomoGeom()
+        g.kind, g.n, g.na, g.nz = self.kind, self.n, self.na, self.nz
+        g.angles = self.angles_c.ctypes.data_as(_f32p)
+        for key, val in extra.items():
+            if isinstance(val, np.ndarray):
+                arr = np.ascontiguousarray(val, dtype=np.float32)
+                self._keep.append(arr)
+                setattr(g, key, arr.ctypes.data_as(_f32p))
+            else:
+                setattr(g, key, val)
+        self._lock = threading.Lock()
+        h = ctypes.c_void_p()
+        check(lib.tomo_plan_create(ctypes.byref(g), ctypes.byref(h)), "tomo_plan_create")
+        self._h = h
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) is not None and self._h.value:
+            lib.tomo_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def image_shape(self):
+        return (self.nz, self.n, self.n)
+
+    @property
+    def sino_shape(self):
+        return (self.nz, self.na, self.n)
+
+    def _run(self, x, fwd: bool):
+        in_shape = self.image_shape if fwd else self.sino_shape
+        out_shape = self.sino_shape if fwd else self.image_shape
+        if isinstance(x, np.ndarray):
+            xin = np.ascontiguousarray(x, dtype=np.float32)
+            if xin.size != int(np.prod(in_shape)):
+                raise ValueError(f"expected {in_shape} elements, got shape {x.shape}")
+            out = np.empty(out_shape, np.float32)
+            fn = lib.tomo_forward_host if fwd else lib.tomo_adjoint_host
+            with self._lock:
+                check(fn(self._h, xin.ctypes.data, out.ctypes.data), "host projector call")
+            return out
+        torch = _torch()
+        if not (isinstance(x, torch.Tensor) and x.is_cuda and x.dtype == torch.float32):
+            raise TypeError("expected a numpy array or a CUDA float32 torch tensor")
+        if x.numel() != int(np.prod(in_shape)):
+            raise ValueError(f"expected {in_shape} elements, got shape {tuple(x.shape)}")
+        xin = x.contiguous()
+        out = torch.empty(out_shape, dtype=torch.float32, device=x.device)
+        stream = torch.cuda.current_stream(x.device).cuda_stream
+        fn = lib.tomo_forward if fwd else lib.tomo_adjoint
+        with self._lock:
+            check(fn(self._h, xin.data_ptr(), out.data_ptr(), stream), "device projector call")
+        return out
+
+    def forward(self, x):
+        return self._run(x, True)
+
+    def adjoint(self, y):
+        return self._run(y, False)

@@ -1,0 +1,247 @@
+// C ABI of libtomo_b200: plans, dispatch, host-buffer calls and the drop-in
+// entry points that mirror the reference C functions (include/tomo_b200.h).
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "tomo_internal.cuh"
+
+namespace tomo {
+
+static thread_local std::string g_last_error;
+
+void set_error(const std::string &msg) { g_last_error = msg; }
+
+int fail(int code, const std::string &msg) {
+  g_last_error = msg;
+  return code;
+}
+
+int cuda_fail(cudaError_t e, const char *what) {
+  g_last_error = std::string("CUDA error ") + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) +
+                 ") in " + what;
+  return TOMO_ECUDA;
+}
+
+size_t image_elems(const Plan &p) { return (size_t)p.g.nz * p.g.n * p.g.n; }
+size_t sino_elems(const Plan &p) { return (size_t)p.g.nz * p.g.na * p.g.n; }
+
+static void release(Plan &p) {
+  if (p.d_angles) cudaFree(p.d_angles);
+  if (p.d_scratch) cudaFree(p.d_scratch);
+  if (p.d_in) cudaFree(p.d_in);
+  if (p.d_out) cudaFree(p.d_out);
+  if (p.host_stream) cudaStreamDestroy(p.host_stream);
+  p.d_angles = nullptr;
+  p.d_scratch = p.d_in = p.d_out = nullptr;
+  p.host_stream = nullptr;
+}
+
+static int validate(const tomo_geom *g) {
+  if (!g) return fail(TOMO_EINVAL, "geometry is NULL");
+  if (g->n < 2 || g->n > 32767)
+    return fail(TOMO_EINVAL, "n (npix) must be in [2, 32767], got " + std::to_string(g->n));
+  if (g->na < 1) return fail(TOMO_EINVAL, "na (nang) must be >= 1, got " + std::to_string(g->na));
+  if (g->nz < 1) return fail(TOMO_EINVAL, "nz must be >= 1, got " + std::to_string(g->nz));
+  if (!g->angles) return fail(TOMO_EINVAL, "angles pointer is NULL");
+  for (int v = 0; v < g->na; ++v)
+    if (!std::isfinite(g->angles[v]))
+      return fail(TOMO_EINVAL, "angle " + std::to_string(v) + " is not finite");
+  switch (g->kind) {
+    case TOMO_KIND_DD:
+      return TOMO_OK;
+    default:
+      return fail(TOMO_EINVAL, "projector kind " + std::to_string(g->kind) + " is not available");
+  }
+}
+
+}  // namespace tomo
+
+using namespace tomo;
+
+struct tomo_plan {
+  Plan p;
+};
+
+extern "C" {
+
+int tomo_last_error(char *buf, size_t len) {
+  if (buf && len) {
+    std::snprintf(buf, len, "%s", g_last_error.c_str());
+  }
+  return TOMO_OK;
+}
+
+const char *tomo_version(void) { return "tomo_b200 0.1 sm_100a"; }
+
+int tomo_plan_create(const tomo_geom *geom, tomo_plan **out) {
+  if (!out) return fail(TOMO_EINVAL, "plan output pointer is NULL");
+  *out = nullptr;
+  int rc = validate(geom);
+  if (rc) return rc;
+  auto *tp = new tomo_plan();
+  Plan &p = tp->p;
+  p.g = *geom;
+  p.nh = (int)(geom->n * 0.5);
+  p.angles.assign(geom->angles, geom->angles + geom->na);
+  p.g.angles = nullptr;
+  cudaGetDevice(&p.device);
+  switch (p.g.kind) {
+    case TOMO_KIND_DD:
+      rc = dd_setup(p);
+      break;
+    default:
+      rc = fail(TOMO_EINVAL, "unsupported kind");
+  }
+  if (rc) {
+    release(p);
+    delete tp;
+    return rc;
+  }
+  *out = tp;
+  return TOMO_OK;
+}
+
+int tomo_plan_destroy(tomo_plan *plan) {
+  if (!plan) return TOMO_OK;
+  release(plan->p);
+  delete plan;
+  return TOMO_OK;
+}
+
+int tomo_forward(tomo_plan *plan, const float *d_image, float *d_sino, void *stream) {
+  if (!plan || !d_image || !d_sino) return fail(TOMO_EINVAL, "tomo_forward: NULL argument");
+  Plan &p = plan->p;
+  cudaStream_t s = (cudaStream_t)stream;
+  switch (p.g.kind) {
+    case TOMO_KIND_DD:
+      return dd_forward(p, d_image, d_sino, s);
+  }
+  return fail(TOMO_EINVAL, "tomo_forward: unsupported kind");
+}
+
+int tomo_adjoint(tomo_plan *plan, const float *d_sino, float *d_image, void *stream) {
+  if (!plan || !d_image || !d_sino) return fail(TOMO_EINVAL, "tomo_adjoint: NULL argument");
+  Plan &p = plan->p;
+  cudaStream_t s = (cudaStream_t)stream;
+  switch (p.g.kind) {
+    case TOMO_KIND_DD:
+      return dd_adjoint(p, d_sino, d_image, s);
+  }
+  return fail(TOMO_EINVAL, "tomo_adjoint: unsupported kind");
+}
+
+static int ensure_host_buffers(Plan &p) {
+  if (!p.host_stream) TOMO_CUDA(cudaStreamCreateWithFlags(&p.host_stream, cudaStreamNonBlocking));
+  const size_t ib = sizeof(float) * image_elems(p), sb = sizeof(float) * sino_elems(p);
+  if (!p.d_in) {
+    TOMO_CUDA(cudaMalloc(&p.d_in, ib > sb ? ib : sb));
+    p.d_in_bytes = ib > sb ? ib : sb;
+  }
+  if (!p.d_out) {
+    TOMO_CUDA(cudaMalloc(&p.d_out, ib > sb ? ib : sb));
+    p.d_out_bytes = ib > sb ? ib : sb;
+  }
+  return TOMO_OK;
+}
+
+static int host_call(tomo_plan *plan, const float *h_in, float *h_out, bool forward) {
+  if (!plan || !h_in || !h_out) return fail(TOMO_EINVAL, "host call: NULL argument");
+  Plan &p = plan->p;
+  int rc = ensure_host_buffers(p);
+  if (rc) return rc;
+  const size_t ib = sizeof(float) * image_elems(p), sb = sizeof(float) * sino_elems(p);
+  const size_t in_b = forward ? ib : sb, out_b = forward ? sb : ib;
+  TOMO_CUDA(cudaMemcpyAsync(p.d_in, h_in, in_b, cudaMemcpyHostToDevice, p.host_stream));
+  rc = forward ? tomo_forward(plan, p.d_in, p.d_out, p.host_stream)
+               : tomo_adjoint(plan, p.d_in, p.d_out, p.host_stream);
+  if (rc) return rc;
+  TOMO_CUDA(cudaMemcpyAsync(h_out, p.d_out, out_b, cudaMemcpyDeviceToHost, p.host_stream));
+  TOMO_CUDA(cudaStreamSynchronize(p.host_stream));
+  return TOMO_OK;
+}
+
+int tomo_forward_host(tomo_plan *plan, const float *h_image, float *h_sino) {
+  return host_call(plan, h_image, h_sino, true);
+}
+
+int tomo_adjoint_host(tomo_plan *plan, const float *h_sino, float *h_image) {
+  return host_call(plan, h_sino, h_image, false);
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Drop-in entry points.  A small cache keeps one plan per (kind, n, angles) so
+// that repeated calls -- the reference solvers call the same projector every
+// iteration -- do not rebuild geometry tables or reallocate buffers.
+// ---------------------------------------------------------------------------
+namespace {
+
+std::mutex g_dropin_mu;
+
+struct CacheKey {
+  int kind, n, na;
+  std::vector<float> angles;
+  bool operator<(const CacheKey &o) const {
+    return std::tie(kind, n, na, angles) < std::tie(o.kind, o.n, o.na, o.angles);
+  }
+};
+
+std::map<CacheKey, tomo_plan *> g_cache;
+
+int cached_plan(int kind, int n, const float *angles, int na, tomo_plan **out) {
+  if (!angles || na < 1) return fail(TOMO_EINVAL, "angles missing");
+  CacheKey key{kind, n, na, std::vector<float>(angles, angles + na)};
+  auto it = g_cache.find(key);
+  if (it != g_cache.end()) {
+    *out = it->second;
+    return TOMO_OK;
+  }
+  if (g_cache.size() >= 16) {
+    for (auto &kv : g_cache) tomo_plan_destroy(kv.second);
+    g_cache.clear();
+  }
+  tomo_geom g{};
+  g.kind = kind;
+  g.n = n;
+  g.na = na;
+  g.nz = 1;
+  g.angles = angles;
+  int rc = tomo_plan_create(&g, out);
+  if (rc) return rc;
+  g_cache[key] = *out;
+  return TOMO_OK;
+}
+
+// out_host += A in_host (oper 0) or A^T (oper 1), like the reference C.
+int dropin_radon(int kind, float *image, int npix, const float *angles, int nang, int oper,
+                 float *sino) {
+  if (!image || !sino) return fail(TOMO_EINVAL, "image/sino pointer is NULL");
+  if (oper != 0 && oper != 1) return fail(TOMO_EINVAL, "oper must be 0 (forward) or 1 (adjoint)");
+  std::lock_guard<std::mutex> lk(g_dropin_mu);
+  tomo_plan *plan = nullptr;
+  int rc = cached_plan(kind, npix, angles, nang, &plan);
+  if (rc) return rc;
+  const size_t ni = (size_t)npix * npix, ns = (size_t)nang * npix;
+  std::vector<float> tmp(oper == 0 ? ns : ni);
+  rc = oper == 0 ? tomo_forward_host(plan, image, tmp.data()) : tomo_adjoint_host(plan, sino, tmp.data());
+  if (rc) return rc;
+  float *dst = oper == 0 ? sino : image;
+  for (size_t i = 0; i < tmp.size(); ++i) dst[i] += tmp[i];
+  return TOMO_OK;
+}
+
+}  // namespace
+
+extern "C" int tomo_radon_dd(float *image, int npix, const float *angles, int nang, int oper,
+                             float *sino) {
+  return dropin_radon(TOMO_KIND_DD, image, npix, angles, nang, oper, sino);
+}

@@ -1,0 +1,72 @@
+// Internal declarations shared by the CUDA translation units of libtomo_b200.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/tomo_b200.h"
+
+namespace tomo {
+
+// ---------------------------------------------------------------------------
+// Error plumbing: every entry point returns an int status; the message of the
+// last failure is kept per host thread.
+// ---------------------------------------------------------------------------
+void set_error(const std::string &msg);
+int fail(int code, const std::string &msg);
+int cuda_fail(cudaError_t e, const char *what);
+
+#define TOMO_CUDA(call)                                  \
+  do {                                                   \
+    cudaError_t e_ = (call);                             \
+    if (e_ != cudaSuccess) return ::tomo::cuda_fail(e_, #call); \
+  } while (0)
+
+// ---------------------------------------------------------------------------
+// Per-angle geometry, evaluated on the host exactly as the compiled reference
+// evaluates it (glibc sincosf, reciprocal products) and uploaded once per plan.
+// ---------------------------------------------------------------------------
+enum DdMode : int {
+  DD_NONE = 0,   // angle contributes nothing (theta == pi/2 exactly; unreachable)
+  DD_ROWSUM = 1, // |sin| < 1e-7: detector i <- sum of image row i      (radon_dd.c:75-84)
+  DD_COLSUM = 2, // |cos| < 1e-7: detector i <- sum of image column i   (radon_dd.c:87-96)
+  DD_ROWS = 3,   // theta > pi/2: lines are image rows                  (radon_dd.c:99-190)
+  DD_COLS = 4,   // 0 < theta < pi/2 or theta < 0: lines are columns    (radon_dd.c:194-283)
+};
+
+struct DdAngle {
+  int mode;     // DdMode
+  int out_row;  // sinogram row written for this angle (na - 1 - v)
+  float r;      // 1/s (ROWS) or 1/c (COLS): detector boundary D_m = (m - nh) * r
+  float k;      // c*r (ROWS) or s*r (COLS): line offset q_i = ((i - nh) + 0.5) * k
+};
+
+struct Plan {
+  tomo_geom g{};
+  int nh = 0;
+  std::vector<float> angles;  // host copy of the angle array
+  // device tables
+  void *d_angles = nullptr;   // kind-specific per-angle table
+  // scratch owned by the plan (e.g. transposed image for the dd forward)
+  float *d_scratch = nullptr;
+  size_t scratch_bytes = 0;
+  // host-call staging
+  float *d_in = nullptr, *d_out = nullptr;  // device buffers for *_host calls
+  size_t d_in_bytes = 0, d_out_bytes = 0;
+  cudaStream_t host_stream = nullptr;
+  int device = 0;
+};
+
+size_t image_elems(const Plan &p);
+size_t sino_elems(const Plan &p);
+
+// Distance-driven pair (radon_dd.cu)
+int dd_setup(Plan &p);
+int dd_forward(Plan &p, const float *d_img, float *d_sino, cudaStream_t s);
+int dd_adjoint(Plan &p, const float *d_sino, float *d_img, cudaStream_t s);
+
+}  // namespace tomo

@@ -1,0 +1,90 @@
+"""Generate the golden fixtures in this directory from the REFERENCE itself.
+
+Run in a tree where the reference C has been compiled into ``oracle/_ref``
+(``make -C oracle ref``):
+
+    python tests/golden/make_golden.py
+
+For every projector pair and a set of small shapes (even and odd sides, dense
+and sparse angle sets, special angles 0/45/90/135 degrees) it draws seeded
+inputs, runs the reference C through a restatement of its Cython shim
+(oracle/oracle.py: RefLib), and stores inputs and outputs (float32) in
+``radon_golden.npz`` / ``bspline_golden.npz``.  The GPU parity tests compare
+the CUDA path against these arrays, so the tests need neither the reference
+tree nor the compiled reference on the machine that runs them.
+"""
+from __future__ import annotations
+
+import sys
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parents[2]
+sys.path.insert(0, str(ROOT))
+
+from oracle.oracle import RefLib, radon_angles  # noqa: E402
+from iterative_tomographic_reconstruction_algorithms_b200.bspline_functions import init_lut_bspline  # noqa: E402
+
+OUT = Path(__file__).resolve().parent
+
+# (name, n, angle set in degrees)
+RADON_CASES = [
+    ("n64_a90", 64, np.linspace(0, 180, 90, endpoint=False)),
+    ("n65_a37", 65, np.linspace(0, 180, 37, endpoint=False)),
+    ("n48_special", 48, np.array([0.0, 30.0, 45.0, 60.0, 90.0, 120.0, 135.0, 150.0, 179.5])),
+    ("n33_a16", 33, np.linspace(0, 180, 16, endpoint=False)),
+    ("n128_a45", 128, np.linspace(0, 180, 45, endpoint=False)),
+]
+
+
+def main() -> None:
+    R = RefLib()
+    rng = np.random.default_rng(20240611)
+    data = {}
+    for name, n, deg in RADON_CASES:
+        ang = radon_angles(deg)
+        na = len(ang)
+        img = rng.standard_normal((n, n)).astype(np.float32)
+        sino = rng.standard_normal((na, n)).astype(np.float32)
+        data[f"{name}/angles_deg"] = deg.astype(np.float64)
+        data[f"{name}/image"] = img
+        data[f"{name}/sino"] = sino
+        for kind in ("pd", "rd", "dd", "ss"):
+            sn = np.abs(np.sin(ang.astype(np.float64)))
+            cs = np.abs(np.cos(ang.astype(np.float64)))
+            nh = n // 2
+            misses = (sn >= 1e-5) & (cs >= 1e-5) & ((nh - 1) * cs + nh * sn < nh + 0.5)
+            if kind == "ss" and np.any(misses):
+                # A ray of radon_ss.c that misses the square [-nh, nh-1]^2
+                # (|sin| * nh < 1 near 180 degrees) makes ray_limits return
+                # limits outside the image and the reference reads/writes out
+                # of bounds (the adjoint corrupts the heap).  No golden values.
+                continue
+            data[f"{name}/{kind}/fwd"] = R.radon(kind, 0, img, ang)
+            data[f"{name}/{kind}/adj"] = R.radon(kind, 1, sino, ang)
+    np.savez_compressed(OUT / "radon_golden.npz", **data)
+
+    data = {}
+    for name, n, na, deg, sup in [("n64_a90_cubic", 64, 90, 3, 4.0), ("n65_a37_cubic", 65, 37, 3, 4.0),
+                                  ("n48_a30_linear", 48, 30, 1, 2.0)]:
+        ang = (np.arange(na) * 180.0) / np.float32(na)  # class_projectors_bspline.py:49-50
+        lut = init_lut_bspline(2048, ang, deg, 1, sup).astype(np.float32)
+        param = np.array([lut.shape[1], sup], np.float32)
+        img = rng.standard_normal((n, n)).astype(np.float32)
+        sino = rng.standard_normal((na, n)).astype(np.float32)
+        a32 = ang.astype(np.float32)
+        data[f"{name}/angles"] = a32
+        data[f"{name}/deg_support"] = np.array([deg, sup], np.float64)
+        data[f"{name}/lut_sum"] = np.array([np.sum(lut, dtype=np.float64)])
+        data[f"{name}/param"] = param
+        data[f"{name}/image"] = img
+        data[f"{name}/sino"] = sino
+        data[f"{name}/fwd"] = R.bspline(0, img, a32, lut, param)
+        data[f"{name}/adj"] = R.bspline(1, sino, a32, lut, param)
+    np.savez_compressed(OUT / "bspline_golden.npz", **data)
+    print("wrote", sorted(p.name for p in OUT.glob("*.npz")))
+
+
+if __name__ == "__main__":
+    main()
