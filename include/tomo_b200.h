@@ -101,11 +101,48 @@ int tomo_adjoint_host(tomo_plan *plan, const float *h_sino, float *h_image);
 
 /* ---- drop-in entry points (reference C signatures; host pointers) ---- */
 
+/* radon_pd.c:20 `void radon_pd(float* image, int npix, float* angles, int nang,
+ * int oper, int method, float* sino)`, bound at radon_pixel_driven.pyx:7-8.
+ * oper 0: sino += A image; oper 1: image += A^T sino.  Only method 1 (linear,
+ * the one class_projectors_radon.py:62 uses) is provided: the reference's
+ * method 0 indexes bins outside [0, npix) for edge pixels; it returns
+ * TOMO_EINVAL. */
+int tomo_radon_pd(float *image, int npix, const float *angles, int nang, int oper,
+                  int method, float *sino);
+
+/* radon_rd.c:76 `void radon_rd(float* image, int npix, float* angles, int nang,
+ * int oper, float* sino)`, bound at radon_ray_driven.pyx:7-8. */
+int tomo_radon_rd(float *image, int npix, const float *angles, int nang, int oper,
+                  float *sino);
+
 /* radon_dd.c:54 `void radon_dd(float* image, int npix, float* angles, int nang,
  * int oper, float* sino)`, bound at radon_distance_driven.pyx:7.  Angles must
  * lie in [-pi/2, pi] (outside it the reference's boundary merge is undefined). */
 int tomo_radon_dd(float *image, int npix, const float *angles, int nang, int oper,
                   float *sino);
+
+/* radon_ss.c:93 `void radon_ss(float* image, int npix, float* angles, int nang,
+ * int oper, int method, float* sino)`, bound at radon_slant_stacking.pyx:7-8.
+ * Only method 1 (linear, class_projectors_radon.py:68) is provided.  Rays that
+ * miss the square [-nh, nh-1]^2 (within about 1/nh rad of 180 degrees) make the
+ * reference index outside the image; here those rows contribute nothing. */
+int tomo_radon_ss(float *image, int npix, const float *angles, int nang, int oper,
+                  int method, float *sino);
+
+/* gen_forwproj.c:22 `void gen_forwproj(float* image, int npix, float* angles,
+ * int nang, float* lut, int lut_size, float support_bspline, int num_cores,
+ * float* sino)`, bound at genradon.pyx:10-11.  Angles in degrees; lut is
+ * [nang][lut_size]; num_cores is accepted and ignored. */
+int tomo_gen_forwproj(const float *image, int npix, const float *angles, int nang,
+                      const float *lut, int lut_size, float support_bspline,
+                      int num_cores, float *sino);
+
+/* gen_backproj.c:22 `void gen_backproj(float* sino, int npix, float* angles,
+ * int nang, float* lut, int lut_size, float support_bspline, float* image)`,
+ * bound at genradon.pyx:13-14. */
+int tomo_gen_backproj(const float *sino, int npix, const float *angles, int nang,
+                      const float *lut, int lut_size, float support_bspline,
+                      float *image);
 
 #ifdef __cplusplus
 }

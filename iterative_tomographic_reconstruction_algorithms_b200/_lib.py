@@ -71,7 +71,13 @@ def _load() -> ctypes.CDLL:
         getattr(lib, name).argtypes = [vp, vp, vp, vp]
     for name in ("tomo_forward_host", "tomo_adjoint_host"):
         getattr(lib, name).argtypes = [vp, vp, vp]
-    lib.tomo_radon_dd.argtypes = [_f32p, i, _f32p, i, i, _f32p]
+    for name in ("tomo_radon_dd", "tomo_radon_rd"):
+        getattr(lib, name).argtypes = [_f32p, i, _f32p, i, i, _f32p]
+    for name in ("tomo_radon_pd", "tomo_radon_ss"):
+        getattr(lib, name).argtypes = [_f32p, i, _f32p, i, i, i, _f32p]
+    lib.tomo_gen_forwproj.argtypes = [_f32p, i, _f32p, i, _f32p, i, f, i, _f32p]
+    lib.tomo_gen_backproj.argtypes = [_f32p, i, _f32p, i, _f32p, i, f, _f32p]
+    lib.tomo_measure_onchip_peaks.argtypes = [ctypes.POINTER(ctypes.c_double)] * 3
     return lib
 
 

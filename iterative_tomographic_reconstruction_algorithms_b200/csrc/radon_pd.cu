@@ -1,0 +1,179 @@
+// Pixel-driven projector pair (linear interpolation, method 1) for sm_100a.
+//
+// Reference: common/operators/radon_module/pymodule_radon_pixel_driven/
+// radon_pd.c:20-90.  Every pixel (i, j) -- stored at image row n-1-i
+// (:61) -- is represented by four sub-samples; the reference offsets x and y by
+// the SAME delta[2k+1] (:42-43), so the four are (-1/4,-1/4) twice and
+// (+1/4,+1/4) twice.  A sub-sample lands at T = nh - t, t = +-|x s - y c| with
+// the sign rule of :46-55, and is split linearly between bins floor(T) and
+// ceil(T) with weights |ceil(T) - T| and |T - floor(T)|; bin 0 never receives
+// (:74,76) and an integral T gets weight 0 in both.  Output row v follows the
+// (fftshifted) angle order of the input.
+//
+// Evaluation order of the compiled reference (-O3 -ffast-math, read from its
+// x86-64 code), reproduced exactly: t = |fma(-c, y, x*s)|, the sign test uses
+// (x*s) * (1/c), and the first weight is |(t + ceil(T)) - nh|.
+//
+// Forward = gather per (angle, bin) over the image strip whose sub-samples land
+// within one bin of it; adjoint = gather per pixel over angles.  The duplicate
+// sub-samples are evaluated once with weight 2 * 1/4.
+#include <cmath>
+
+#include "tomo_internal.cuh"
+
+namespace tomo {
+namespace {
+
+constexpr double kPi = 3.141592653589793;
+
+struct PdEval {
+  float wl, wu;  // weights of bins l = floor(T), u = ceil(T)
+  int l, u;      // -1 when the reference's bound test (0 < bin < n) fails
+};
+
+__device__ __forceinline__ PdEval pd_eval(float x, float y, const PdAngle &g, float fnh, int n) {
+  const float xs = __fmul_rn(x, g.s);
+  const float t = fabsf(__fmaf_rn(-g.c, y, xs));
+  const float r = __fmul_rn(xs, g.rc);
+  const bool keep = ((g.flags & 1) && y > r) || ((g.flags & 2) && y > r) || ((g.flags & 4) && y > 0.0f);
+  const float ts = keep ? t : -t;
+  const float T = __fsub_rn(fnh, ts);
+  const float lf = floorf(T), uf = ceilf(T);
+  PdEval e;
+  e.wl = fabsf(__fsub_rn(__fadd_rn(ts, uf), fnh));
+  e.wu = fabsf(__fsub_rn(T, lf));
+  e.l = (lf >= 1.0f && lf < (float)n) ? (int)lf : -1;
+  e.u = (uf >= 1.0f && uf < (float)n) ? (int)uf : -1;
+  return e;
+}
+
+// Forward: thread per (bin b, angle v, slice).  Iterates the lines of the
+// axis along which the projection moves fastest, and per line only the pixels
+// whose sub-samples can land in (b-1, b+1).
+__global__ void __launch_bounds__(128) pd_forward_kernel(
+    const float *__restrict__ img, float *__restrict__ sino, const PdAngle *__restrict__ tab,
+    int n, int nh, int na) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  const int v = blockIdx.y;
+  const size_t z = blockIdx.z;
+  if (b >= n) return;
+  const PdAngle g = tab[v];
+  const float *I = img + z * (size_t)n * n;
+  const float fnh = (float)nh;
+  float acc = 0.0f;
+  if (b >= 1) {
+    // T ~ nh - sigma*((y0+d) c - (x0+d) s), sigma = sign(c)
+    const float sg = g.c >= 0.0f ? 1.0f : -1.0f;
+    const bool by_rows = fabsf(g.s) >= fabsf(g.c);
+    for (int line = 0; line < n; ++line) {
+      const float o0 = (float)line - fnh + 0.5f;  // y0 (rows) or x0 (columns)
+      float lo = 1e30f, hi = -1e30f;
+      for (int e = 0; e < 2; ++e) {
+        const float d = e ? 0.25f : -0.25f;
+        for (int f = 0; f < 2; ++f) {
+          const float T = (float)(b - 1 + 2 * f);
+          float w;  // the other pixel-centre coordinate giving this T
+          if (by_rows) w = (T - fnh + sg * ((o0 + d) * g.c)) / (sg * g.s) - d;
+          else w = (fnh - T + sg * ((o0 + d) * g.s)) / (sg * g.c) - d;
+          lo = fminf(lo, w);
+          hi = fmaxf(hi, w);
+        }
+      }
+      int j0 = (int)floorf(lo + fnh - 0.5f) - 1, j1 = (int)ceilf(hi + fnh - 0.5f) + 1;
+      j0 = max(j0, 0);
+      j1 = min(j1, n - 1);
+      for (int j = j0; j <= j1; ++j) {
+        const int ii = by_rows ? line : j, jj = by_rows ? j : line;
+        const float x0 = (float)jj - fnh + 0.5f, y0 = (float)ii - fnh + 0.5f;
+        const float val = __ldg(I + (size_t)(n - 1 - ii) * n + jj);
+        float wsum = 0.0f;
+        for (int e = 0; e < 2; ++e) {
+          const float d = e ? 0.25f : -0.25f;
+          const PdEval q = pd_eval(__fadd_rn(x0, d), __fadd_rn(y0, d), g, fnh, n);
+          if (q.l == b) wsum += q.wl;
+          if (q.u == b) wsum += q.wu;
+        }
+        if (wsum != 0.0f) acc = fmaf(0.5f * wsum, val, acc);
+      }
+    }
+  }
+  sino[z * (size_t)na * n + (size_t)v * n + b] = acc;
+}
+
+constexpr int kPdChunk = 1024;
+
+// Adjoint: thread per output pixel (memory row R, column j); the reference's
+// loop row is i = n-1-R.
+__global__ void __launch_bounds__(256) pd_adjoint_kernel(
+    const float *__restrict__ sino, float *__restrict__ img, const PdAngle *__restrict__ tab,
+    int n, int nh, int na) {
+  __shared__ PdAngle stab[kPdChunk];
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  const int R = blockIdx.y * blockDim.y + threadIdx.y;
+  const size_t z = blockIdx.z;
+  const bool live = R < n && j < n;
+  const float *S = sino + z * (size_t)na * n;
+  const int tid = threadIdx.y * blockDim.x + threadIdx.x, nthr = blockDim.x * blockDim.y;
+  const float fnh = (float)nh;
+  const int i = n - 1 - R;
+  const float x0 = (float)j - fnh + 0.5f, y0 = (float)i - fnh + 0.5f;
+  float acc = 0.0f;
+  for (int v0 = 0; v0 < na; v0 += kPdChunk) {
+    const int cnt = min(kPdChunk, na - v0);
+    __syncthreads();
+    for (int t = tid; t < cnt; t += nthr) stab[t] = tab[v0 + t];
+    __syncthreads();
+    if (!live) continue;
+    for (int u = 0; u < cnt; ++u) {
+      const PdAngle g = stab[u];
+      const float *row = S + (size_t)(v0 + u) * n;
+      for (int e = 0; e < 2; ++e) {
+        const float d = e ? 0.25f : -0.25f;
+        const PdEval q = pd_eval(__fadd_rn(x0, d), __fadd_rn(y0, d), g, fnh, n);
+        if (q.l >= 0) acc = fmaf(0.5f * q.wl, __ldg(row + q.l), acc);
+        if (q.u >= 0) acc = fmaf(0.5f * q.wu, __ldg(row + q.u), acc);
+      }
+    }
+  }
+  if (live) img[z * (size_t)n * n + (size_t)R * n + j] = acc;
+}
+
+}  // namespace
+
+int pd_setup(Plan &p) {
+  const int na = p.g.na;
+  std::vector<PdAngle> tab(na);
+  for (int v = 0; v < na; ++v) {
+    const float theta = p.angles[v];
+    float s, c;
+    sincosf(theta, &s, &c);
+    PdAngle a{};
+    a.s = s;
+    a.c = c;
+    a.rc = 1.0f / c;
+    a.flags = ((double)theta < kPi / 2 ? 1 : 0) | ((double)theta > kPi / 2 ? 2 : 0) |
+              (theta == 0.0f ? 4 : 0);
+    tab[v] = a;
+  }
+  TOMO_CUDA(cudaMalloc(&p.d_angles, sizeof(PdAngle) * (size_t)na));
+  TOMO_CUDA(cudaMemcpy(p.d_angles, tab.data(), sizeof(PdAngle) * (size_t)na, cudaMemcpyHostToDevice));
+  return TOMO_OK;
+}
+
+int pd_forward(Plan &p, const float *d_img, float *d_sino, cudaStream_t s) {
+  const int n = p.g.n, na = p.g.na, nz = p.g.nz;
+  dim3 fb(128), fg((n + 127) / 128, na, nz);
+  pd_forward_kernel<<<fg, fb, 0, s>>>(d_img, d_sino, (const PdAngle *)p.d_angles, n, p.nh, na);
+  TOMO_CUDA(cudaGetLastError());
+  return TOMO_OK;
+}
+
+int pd_adjoint(Plan &p, const float *d_sino, float *d_img, cudaStream_t s) {
+  const int n = p.g.n, na = p.g.na, nz = p.g.nz;
+  dim3 ab(32, 8), ag((n + 31) / 32, (n + 7) / 8, nz);
+  pd_adjoint_kernel<<<ag, ab, 0, s>>>(d_sino, d_img, (const PdAngle *)p.d_angles, n, p.nh, na);
+  TOMO_CUDA(cudaGetLastError());
+  return TOMO_OK;
+}
+
+}  // namespace tomo

@@ -35,11 +35,12 @@ size_t sino_elems(const Plan &p) { return (size_t)p.g.nz * p.g.na * p.g.n; }
 
 static void release(Plan &p) {
   if (p.d_angles) cudaFree(p.d_angles);
+  if (p.d_aux) cudaFree(p.d_aux);
   if (p.d_scratch) cudaFree(p.d_scratch);
   if (p.d_in) cudaFree(p.d_in);
   if (p.d_out) cudaFree(p.d_out);
   if (p.host_stream) cudaStreamDestroy(p.host_stream);
-  p.d_angles = nullptr;
+  p.d_angles = p.d_aux = nullptr;
   p.d_scratch = p.d_in = p.d_out = nullptr;
   p.host_stream = nullptr;
 }
@@ -48,14 +49,20 @@ static int validate(const tomo_geom *g) {
   if (!g) return fail(TOMO_EINVAL, "geometry is NULL");
   if (g->n < 2 || g->n > 32767)
     return fail(TOMO_EINVAL, "n (npix) must be in [2, 32767], got " + std::to_string(g->n));
-  if (g->na < 1) return fail(TOMO_EINVAL, "na (nang) must be >= 1, got " + std::to_string(g->na));
-  if (g->nz < 1) return fail(TOMO_EINVAL, "nz must be >= 1, got " + std::to_string(g->nz));
+  if (g->na < 1 || g->na > 65535)
+    return fail(TOMO_EINVAL, "na (nang) must be in [1, 65535], got " + std::to_string(g->na));
+  if (g->nz < 1 || g->nz > 65535)
+    return fail(TOMO_EINVAL, "nz must be in [1, 65535], got " + std::to_string(g->nz));
   if (!g->angles) return fail(TOMO_EINVAL, "angles pointer is NULL");
   for (int v = 0; v < g->na; ++v)
     if (!std::isfinite(g->angles[v]))
       return fail(TOMO_EINVAL, "angle " + std::to_string(v) + " is not finite");
   switch (g->kind) {
+    case TOMO_KIND_PD:
+    case TOMO_KIND_RD:
     case TOMO_KIND_DD:
+    case TOMO_KIND_SS:
+    case TOMO_KIND_BSPLINE:
       return TOMO_OK;
     default:
       return fail(TOMO_EINVAL, "projector kind " + std::to_string(g->kind) + " is not available");
@@ -94,9 +101,11 @@ int tomo_plan_create(const tomo_geom *geom, tomo_plan **out) {
   p.g.angles = nullptr;
   cudaGetDevice(&p.device);
   switch (p.g.kind) {
-    case TOMO_KIND_DD:
-      rc = dd_setup(p);
-      break;
+    case TOMO_KIND_PD: rc = pd_setup(p); break;
+    case TOMO_KIND_RD: rc = rd_setup(p); break;
+    case TOMO_KIND_DD: rc = dd_setup(p); break;
+    case TOMO_KIND_SS: rc = ss_setup(p); break;
+    case TOMO_KIND_BSPLINE: rc = bs_setup(p); break;
     default:
       rc = fail(TOMO_EINVAL, "unsupported kind");
   }
@@ -121,8 +130,11 @@ int tomo_forward(tomo_plan *plan, const float *d_image, float *d_sino, void *str
   Plan &p = plan->p;
   cudaStream_t s = (cudaStream_t)stream;
   switch (p.g.kind) {
-    case TOMO_KIND_DD:
-      return dd_forward(p, d_image, d_sino, s);
+    case TOMO_KIND_PD: return pd_forward(p, d_image, d_sino, s);
+    case TOMO_KIND_RD: return rd_forward(p, d_image, d_sino, s);
+    case TOMO_KIND_DD: return dd_forward(p, d_image, d_sino, s);
+    case TOMO_KIND_SS: return ss_forward(p, d_image, d_sino, s);
+    case TOMO_KIND_BSPLINE: return bs_forward(p, d_image, d_sino, s);
   }
   return fail(TOMO_EINVAL, "tomo_forward: unsupported kind");
 }
@@ -132,8 +144,11 @@ int tomo_adjoint(tomo_plan *plan, const float *d_sino, float *d_image, void *str
   Plan &p = plan->p;
   cudaStream_t s = (cudaStream_t)stream;
   switch (p.g.kind) {
-    case TOMO_KIND_DD:
-      return dd_adjoint(p, d_sino, d_image, s);
+    case TOMO_KIND_PD: return pd_adjoint(p, d_sino, d_image, s);
+    case TOMO_KIND_RD: return rd_adjoint(p, d_sino, d_image, s);
+    case TOMO_KIND_DD: return dd_adjoint(p, d_sino, d_image, s);
+    case TOMO_KIND_SS: return ss_adjoint(p, d_sino, d_image, s);
+    case TOMO_KIND_BSPLINE: return bs_adjoint(p, d_sino, d_image, s);
   }
   return fail(TOMO_EINVAL, "tomo_adjoint: unsupported kind");
 }
@@ -190,16 +205,23 @@ std::mutex g_dropin_mu;
 struct CacheKey {
   int kind, n, na;
   std::vector<float> angles;
+  std::vector<float> extra;  // B-spline LUT and support
   bool operator<(const CacheKey &o) const {
-    return std::tie(kind, n, na, angles) < std::tie(o.kind, o.n, o.na, o.angles);
+    return std::tie(kind, n, na, angles, extra) < std::tie(o.kind, o.n, o.na, o.angles, o.extra);
   }
 };
 
 std::map<CacheKey, tomo_plan *> g_cache;
 
-int cached_plan(int kind, int n, const float *angles, int na, tomo_plan **out) {
+int cached_plan(int kind, int n, const float *angles, int na, tomo_plan **out,
+                const float *lut = nullptr, int lut_size = 0, float support = 0.0f) {
   if (!angles || na < 1) return fail(TOMO_EINVAL, "angles missing");
-  CacheKey key{kind, n, na, std::vector<float>(angles, angles + na)};
+  CacheKey key{kind, n, na, std::vector<float>(angles, angles + na), {}};
+  if (lut) {
+    key.extra.assign(lut, lut + (size_t)na * lut_size);
+    key.extra.push_back(support);
+    key.extra.push_back((float)lut_size);
+  }
   auto it = g_cache.find(key);
   if (it != g_cache.end()) {
     *out = it->second;
@@ -215,6 +237,9 @@ int cached_plan(int kind, int n, const float *angles, int na, tomo_plan **out) {
   g.na = na;
   g.nz = 1;
   g.angles = angles;
+  g.lut = lut;
+  g.lut_size = lut_size;
+  g.support = support;
   int rc = tomo_plan_create(&g, out);
   if (rc) return rc;
   g_cache[key] = *out;
@@ -223,12 +248,12 @@ int cached_plan(int kind, int n, const float *angles, int na, tomo_plan **out) {
 
 // out_host += A in_host (oper 0) or A^T (oper 1), like the reference C.
 int dropin_radon(int kind, float *image, int npix, const float *angles, int nang, int oper,
-                 float *sino) {
+                 float *sino, const float *lut = nullptr, int lut_size = 0, float support = 0.0f) {
   if (!image || !sino) return fail(TOMO_EINVAL, "image/sino pointer is NULL");
   if (oper != 0 && oper != 1) return fail(TOMO_EINVAL, "oper must be 0 (forward) or 1 (adjoint)");
   std::lock_guard<std::mutex> lk(g_dropin_mu);
   tomo_plan *plan = nullptr;
-  int rc = cached_plan(kind, npix, angles, nang, &plan);
+  int rc = cached_plan(kind, npix, angles, nang, &plan, lut, lut_size, support);
   if (rc) return rc;
   const size_t ni = (size_t)npix * npix, ns = (size_t)nang * npix;
   std::vector<float> tmp(oper == 0 ? ns : ni);
@@ -244,4 +269,41 @@ int dropin_radon(int kind, float *image, int npix, const float *angles, int nang
 extern "C" int tomo_radon_dd(float *image, int npix, const float *angles, int nang, int oper,
                              float *sino) {
   return dropin_radon(TOMO_KIND_DD, image, npix, angles, nang, oper, sino);
+}
+
+extern "C" int tomo_radon_rd(float *image, int npix, const float *angles, int nang, int oper,
+                             float *sino) {
+  return dropin_radon(TOMO_KIND_RD, image, npix, angles, nang, oper, sino);
+}
+
+extern "C" int tomo_radon_pd(float *image, int npix, const float *angles, int nang, int oper,
+                             int method, float *sino) {
+  if (method != 1)
+    return fail(TOMO_EINVAL, "radon_pd: only method 1 (linear interpolation) is provided; the "
+                             "reference's method 0 writes outside the sinogram for edge pixels");
+  return dropin_radon(TOMO_KIND_PD, image, npix, angles, nang, oper, sino);
+}
+
+extern "C" int tomo_radon_ss(float *image, int npix, const float *angles, int nang, int oper,
+                             int method, float *sino) {
+  if (method != 1)
+    return fail(TOMO_EINVAL, "radon_ss: only method 1 (linear interpolation) is provided");
+  return dropin_radon(TOMO_KIND_SS, image, npix, angles, nang, oper, sino);
+}
+
+extern "C" int tomo_gen_forwproj(const float *image, int npix, const float *angles, int nang,
+                                 const float *lut, int lut_size, float support_bspline,
+                                 int num_cores, float *sino) {
+  (void)num_cores;
+  if (!lut) return fail(TOMO_EINVAL, "gen_forwproj: lut is NULL");
+  return dropin_radon(TOMO_KIND_BSPLINE, const_cast<float *>(image), npix, angles, nang, 0, sino,
+                      lut, lut_size, support_bspline);
+}
+
+extern "C" int tomo_gen_backproj(const float *sino, int npix, const float *angles, int nang,
+                                 const float *lut, int lut_size, float support_bspline,
+                                 float *image) {
+  if (!lut) return fail(TOMO_EINVAL, "gen_backproj: lut is NULL");
+  return dropin_radon(TOMO_KIND_BSPLINE, image, npix, angles, nang, 1, const_cast<float *>(sino),
+                      lut, lut_size, support_bspline);
 }

@@ -45,12 +45,36 @@ struct DdAngle {
   float k;      // c*r (ROWS) or s*r (COLS): line offset q_i = ((i - nh) + 0.5) * k
 };
 
+// Slant stacking (radon_ss.c): steep rays step y and interpolate x.
+struct SsAngle {
+  int out_row;  // na - 1 - v
+  int steep;    // |sin| <= sqrt(1/2)
+  float a;      // minor coordinate f = fma(-m, a, t) * rb: a = s (steep) or c
+  float rb;     // 1/c (steep) or 1/s
+  float wt;     // 1/|c| (steep) or 1/|s|
+};
+
+// Pixel-driven (radon_pd.c).
+struct PdAngle {
+  float s, c, rc;  // sin, cos, 1/c
+  int flags;       // 1: theta < pi/2, 2: theta > pi/2, 4: theta == 0
+};
+
+// Ray-driven / Siddon (radon_rd.c).
+struct RdAngle {
+  float s, c, rc, rs;      // sin, cos, 1/c, 1/s
+  float ns, nc, mns, mnc;  // nh*s, nh*c, -nh*s, -nh*c
+  int mode;                // 0 general, 1 |s| < 1e-7, 2 |c| < 1e-7
+  int lt, gt;              // theta < pi/2, theta > pi/2
+};
+
 struct Plan {
   tomo_geom g{};
   int nh = 0;
   std::vector<float> angles;  // host copy of the angle array
   // device tables
   void *d_angles = nullptr;   // kind-specific per-angle table
+  void *d_aux = nullptr;      // kind-specific extra table (ss ray limits, B-spline LUT)
   // scratch owned by the plan (e.g. transposed image for the dd forward)
   float *d_scratch = nullptr;
   size_t scratch_bytes = 0;
@@ -64,9 +88,16 @@ struct Plan {
 size_t image_elems(const Plan &p);
 size_t sino_elems(const Plan &p);
 
-// Distance-driven pair (radon_dd.cu)
-int dd_setup(Plan &p);
-int dd_forward(Plan &p, const float *d_img, float *d_sino, cudaStream_t s);
-int dd_adjoint(Plan &p, const float *d_sino, float *d_img, cudaStream_t s);
+// One setup/forward/adjoint triple per projector kind.
+#define TOMO_DECLARE_KIND(k)                                                  \
+  int k##_setup(Plan &p);                                                     \
+  int k##_forward(Plan &p, const float *d_img, float *d_sino, cudaStream_t s); \
+  int k##_adjoint(Plan &p, const float *d_sino, float *d_img, cudaStream_t s);
+TOMO_DECLARE_KIND(dd)  // radon_dd.cu
+TOMO_DECLARE_KIND(ss)  // radon_ss.cu
+TOMO_DECLARE_KIND(pd)  // radon_pd.cu
+TOMO_DECLARE_KIND(rd)  // radon_rd.cu
+TOMO_DECLARE_KIND(bs)  // bspline.cu
+#undef TOMO_DECLARE_KIND
 
 }  // namespace tomo

@@ -20,7 +20,7 @@ from oracle.oracle import radon_angles
 
 pytestmark = pytest.mark.gpu
 
-KINDS = ("dd",)
+KINDS = ("pd", "rd", "dd", "ss")
 TOL = 1e-5
 
 
@@ -115,7 +115,9 @@ def test_dropin_entry_point_accumulates(cuda, radon_golden, kind):
     fp = ctypes.POINTER(ctypes.c_float)
     sino = np.ones((len(ang), n), np.float32)
     fn = getattr(_lib.lib, f"tomo_radon_{kind}")
-    rc = fn(img.ctypes.data_as(fp), n, ang.ctypes.data_as(fp), len(ang), 0, sino.ctypes.data_as(fp))
+    extra = (1,) if kind in ("pd", "ss") else ()  # method 1 = linear interpolation
+    rc = fn(img.ctypes.data_as(fp), n, ang.ctypes.data_as(fp), len(ang), 0, *extra,
+            sino.ctypes.data_as(fp))
     assert rc == 0, _lib.last_error()
     assert rel_l2(sino - 1.0, radon_golden[f"{case}/{kind}/fwd"]) <= TOL
 
