@@ -99,6 +99,19 @@ int tomo_adjoint(tomo_plan *plan, const float *d_sino, float *d_image, void *str
 int tomo_forward_host(tomo_plan *plan, const float *h_image, float *h_sino);
 int tomo_adjoint_host(tomo_plan *plan, const float *h_sino, float *h_image);
 
+/* Distance-driven forward projection that allocates no device memory, for
+ * callers that cannot call cudaMalloc (their device memory belongs to another
+ * allocator, or they must not allocate inside a latency-bound loop).  No
+ * counterpart in the reference.  d_image [nz][npix][npix] and d_sino
+ * [nz][nang][npix] are device pointers (the sinogram is overwritten); angles is
+ * the host array tomo_radon_dd receives.  Scratch lives in static device arrays
+ * of this library (16 MiB + 256 KiB per GPU, held until exit): nz*npix*npix
+ * must be <= 4194304 and nang <= 16384, else TOMO_EINVAL.  The first call on a
+ * device sets up the arrays' addresses; make it before any stream capture.
+ * All calls share the arrays: calls that overlap on the GPU race. */
+int tomo_radon_dd_forward_noalloc(const float *d_image, int npix, const float *angles, int nang,
+                                  int nz, float *d_sino, void *stream);
+
 /* ---- drop-in entry points (reference C signatures; host pointers) ---- */
 
 /* radon_pd.c:20 `void radon_pd(float* image, int npix, float* angles, int nang,

@@ -238,6 +238,53 @@ int dd_forward(Plan &p, const float *d_img, float *d_sino, cudaStream_t s) {
   return TOMO_OK;
 }
 
+// Per-angle table for a plan-less caller: same arithmetic as dd_setup.
+int dd_build_table(const float *angles, int na, DdAngle *tab) {
+  for (int v = 0; v < na; ++v) {
+    const float theta = angles[v];
+    float s, c;
+    sincosf(theta, &s, &c);
+    DdAngle a{};
+    a.out_row = na - 1 - v;
+    if (std::fabs((double)s) < 1e-7) {
+      a.mode = DD_ROWSUM;
+    } else if (std::fabs((double)c) < 1e-7) {
+      a.mode = DD_COLSUM;
+    } else if ((double)theta > kPi / 2) {
+      if (!(s > 0.0f))
+        return fail(TOMO_EINVAL, "dd: angle " + std::to_string(theta) +
+                                     " rad is outside [-pi/2, pi], where the reference merge is undefined");
+      a.mode = DD_ROWS;
+      a.r = 1.0f / s;
+      a.k = c * a.r;
+    } else if ((double)theta < kPi / 2 && theta != 0.0f) {
+      if (!(c > 0.0f))
+        return fail(TOMO_EINVAL, "dd: angle " + std::to_string(theta) +
+                                     " rad is outside [-pi/2, pi], where the reference merge is undefined");
+      a.mode = DD_COLS;
+      a.r = 1.0f / c;
+      a.k = s * a.r;
+    } else {
+      a.mode = DD_NONE;
+    }
+    tab[v] = a;
+  }
+  return TOMO_OK;
+}
+
+// Forward launch with caller-provided scratch (>= nz*n*n floats) and device table.
+int dd_forward_launch(const float *d_img, float *d_scratch, float *d_sino, const DdAngle *d_tab,
+                      int n, int na, int nz, cudaStream_t s) {
+  const int nh = (int)(n * 0.5);
+  const size_t stride = (size_t)n * n;
+  dim3 tb(32, 8), tg((n + 31) / 32, (n + 31) / 32, nz);
+  transpose_kernel<<<tg, tb, 0, s>>>(d_img, d_scratch, n, stride);
+  dim3 fb(128), fg((n + 127) / 128, na, nz);
+  dd_forward_kernel<<<fg, fb, 0, s>>>(d_img, d_scratch, d_sino, d_tab, n, nh, na);
+  TOMO_CUDA(cudaGetLastError());
+  return TOMO_OK;
+}
+
 int dd_adjoint(Plan &p, const float *d_sino, float *d_img, cudaStream_t s) {
   const int n = p.g.n, na = p.g.na, nz = p.g.nz;
   dim3 ab(32, 8), ag((n + 31) / 32, (n + 7) / 8, nz);

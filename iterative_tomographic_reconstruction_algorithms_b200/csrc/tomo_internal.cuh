@@ -100,4 +100,9 @@ TOMO_DECLARE_KIND(rd)  // radon_rd.cu
 TOMO_DECLARE_KIND(bs)  // bspline.cu
 #undef TOMO_DECLARE_KIND
 
+// Plan-less pieces of the dd forward (radon_dd.cu), used by dd_noalloc.cu.
+int dd_build_table(const float *angles, int na, DdAngle *tab);
+int dd_forward_launch(const float *d_img, float *d_scratch, float *d_sino, const DdAngle *d_tab,
+                      int n, int na, int nz, cudaStream_t s);
+
 }  // namespace tomo
