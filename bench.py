@@ -45,6 +45,10 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-sample-angles", type=int, default=0,
                     help="angles per step of the CPU baseline sample (0: auto)")
+    ap.add_argument("--profile", action="store_true",
+                    help="run only warm-up + steps of the device path (for ncu captures)")
+    ap.add_argument("--n", type=int, default=N_SIDE, help="image side (profiling only)")
+    ap.add_argument("--na", type=int, default=N_ANG, help="angle count (profiling only)")
     return ap.parse_args()
 
 
@@ -182,13 +186,20 @@ def main():
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
 
-    n, na = N_SIDE, N_ANG
+    n, na = (args.n, args.na) if args.profile else (N_SIDE, N_ANG)
     deg = angles_deg(na)
     tp = cpr.projectors(n, deg, oper="dd")
     img_np = random_ellipses(n, seed=1000 + rank)
     x = torch.from_numpy(img_np).to(dev)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MiB > L2
     stream = torch.cuda.current_stream(dev)
+
+    if args.profile:
+        for _ in range(args.warmup + args.steps):
+            flush.fill_(1.0)
+            tp.At(tp.A(x))
+        torch.cuda.synchronize()
+        return
 
     import ctypes
     s_gbs, l1_gbs, f_tf = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
