@@ -99,6 +99,28 @@ int tomo_adjoint(tomo_plan *plan, const float *d_sino, float *d_image, void *str
 int tomo_forward_host(tomo_plan *plan, const float *h_image, float *h_sino);
 int tomo_adjoint_host(tomo_plan *plan, const float *h_sino, float *h_image);
 
+/* ---- iterative solvers with the update fused into the projector kernels ---- */
+#define TOMO_ALGO_SIRT 1 /* art.py:211-237: x += C A^T(R (b - A x)), R = 1/A1, C = 1/A^T1 */
+#define TOMO_ALGO_MLEM 2 /* sir.py:204-290: x *= (1/A^T1) A^T(b / A x) */
+#define TOMO_ALGO_SPS 3  /* sir.py:348-540 (no penalty): x = clip(x - A^T(w(Ax-b))/(A^T(w A1)+eps), 0, max x) */
+
+typedef struct tomo_solver tomo_solver;
+
+/* Binds a solver to a plan and a measured sinogram d_b [nz][na][n] (device;
+ * must stay valid while the solver lives) and precomputes its normalisation
+ * (R, C; 1/A^T1; w and A^T(w A1)) exactly as the reference does in float32.
+ * Replaces the set-up half of the reference's art.sirt / sir.em / sir.sps. */
+int tomo_solver_create(tomo_plan *plan, int algo, const float *d_b, void *stream,
+                       tomo_solver **solver);
+/* Runs `iters` iterations in place on d_x [nz][n][n].  Each iteration is one
+ * forward and one adjoint launch (plus a residual reduction), captured once
+ * into a CUDA graph when use_graph != 0.  If residuals != NULL it receives
+ * ||A x_k - b||^2 of the iterate entering iteration k (k = 0..iters-1).  The
+ * work is ordered after, and before later work on, `stream`. */
+int tomo_solver_run(tomo_solver *solver, float *d_x, int iters, double *residuals, int use_graph,
+                    void *stream);
+int tomo_solver_destroy(tomo_solver *solver);
+
 /* Distance-driven forward projection that allocates no device memory, for
  * callers that cannot call cudaMalloc (their device memory belongs to another
  * allocator, or they must not allocate inside a latency-bound loop).  No

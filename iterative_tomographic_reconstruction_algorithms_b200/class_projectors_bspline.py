@@ -64,6 +64,10 @@ class projectors:
             self._plans[key] = p
         return p
 
+    def plan(self, nz: int = 1, device=None):
+        """The libtomo_b200 plan (table of Radon degree ``radon_degree``) for ``nz`` slices."""
+        return self._plan(nz, device, "lut")
+
     def _apply(self, x, forward: bool, which: str = "lut"):
         if isinstance(x, np.ndarray) or not hasattr(x, "is_cuda"):
             x = np.asarray(x).astype(myfloat)

@@ -74,6 +74,10 @@ class projectors:
             self._plans[key] = p
         return p
 
+    def plan(self, nz: int = 1, device=None):
+        """The libtomo_b200 plan for ``nz`` slices on CUDA device ``device`` (None: host calls)."""
+        return self._plan(nz, device)
+
     def _apply(self, x, forward: bool):
         is_np = isinstance(x, np.ndarray) or not hasattr(x, "is_cuda")
         if is_np:

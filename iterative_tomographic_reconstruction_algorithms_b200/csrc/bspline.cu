@@ -40,12 +40,12 @@ __device__ __forceinline__ int bs_lut(int yi, float ps, const BsConst &k) {
 
 __global__ void __launch_bounds__(128) bs_forward_kernel(
     const float *__restrict__ img, float *__restrict__ sino, const float2 *__restrict__ cs,
-    const float *__restrict__ lut, BsConst k) {
+    const float *__restrict__ lut, BsConst k, FwdEpi ep) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   const int v = blockIdx.y;
   const size_t z = blockIdx.z;
   const int n = k.n;
-  if (b >= n) return;
+  const bool live = b < n;
   const float C = cs[v].x, S = cs[v].y;
   const float *I = img + z * (size_t)n * n;
   const float *L = lut + (size_t)v * k.lut_size;
@@ -53,7 +53,7 @@ __global__ void __launch_bounds__(128) bs_forward_kernel(
   // taps reach bin b when b <= ps + s + mid < b + 1 (b = 0 also takes (-1, 0))
   const float plo = (float)(b - k.ds - 2) - k.fmid, phi = (float)(b + k.ds + 2) - k.fmid;
   float acc = 0.0f;
-  for (int line = 0; line < n; ++line) {
+  for (int line = 0; line < (live ? n : 0); ++line) {
     // by rows: ky fixed, ps = kx*C + S*ky; by columns: kx fixed, ps = ky*S + kx*C
     const float fixed = by_rows ? (float)(-line + k.mid) : (float)(line - k.mid);
     const float slope = by_rows ? C : S;
@@ -84,14 +84,14 @@ __global__ void __launch_bounds__(128) bs_forward_kernel(
       }
     }
   }
-  sino[z * (size_t)k.na * n + (size_t)v * n + b] = acc;
+  fwd_store(ep, acc, live, z * (size_t)k.na * n + (size_t)v * n + (live ? b : 0), sino);
 }
 
 constexpr int kBsChunk = 1024;
 
 __global__ void __launch_bounds__(256) bs_adjoint_kernel(
     const float *__restrict__ sino, float *__restrict__ img, const float2 *__restrict__ cs,
-    const float *__restrict__ lut, BsConst k) {
+    const float *__restrict__ lut, BsConst k, AdjEpi ep) {
   __shared__ float2 scs[kBsChunk];
   const int n = k.n;
   const int kxi = blockIdx.x * blockDim.x + threadIdx.x;
@@ -122,7 +122,7 @@ __global__ void __launch_bounds__(256) bs_adjoint_kernel(
       }
     }
   }
-  if (live) img[z * (size_t)n * n + (size_t)kyi * n + kxi] = acc;
+  adj_store(ep, acc, live, z * (size_t)n * n + (size_t)(live ? kyi : 0) * n + (live ? kxi : 0), img);
 }
 
 BsConst make_const(const Plan &p) {
@@ -163,20 +163,20 @@ int bs_setup(Plan &p) {
   return TOMO_OK;
 }
 
-int bs_forward(Plan &p, const float *d_img, float *d_sino, cudaStream_t s) {
+int bs_forward(Plan &p, const float *d_img, float *d_sino, cudaStream_t s, const FwdEpi &ep) {
   const BsConst k = make_const(p);
   dim3 fb(128), fg((k.n + 127) / 128, k.na, p.g.nz);
   bs_forward_kernel<<<fg, fb, 0, s>>>(d_img, d_sino, (const float2 *)p.d_angles,
-                                      (const float *)p.d_aux, k);
+                                      (const float *)p.d_aux, k, ep);
   TOMO_CUDA(cudaGetLastError());
   return TOMO_OK;
 }
 
-int bs_adjoint(Plan &p, const float *d_sino, float *d_img, cudaStream_t s) {
+int bs_adjoint(Plan &p, const float *d_sino, float *d_img, cudaStream_t s, const AdjEpi &ep) {
   const BsConst k = make_const(p);
   dim3 ab(32, 8), ag((k.n + 31) / 32, (k.n + 7) / 8, p.g.nz);
   bs_adjoint_kernel<<<ag, ab, 0, s>>>(d_sino, d_img, (const float2 *)p.d_angles,
-                                      (const float *)p.d_aux, k);
+                                      (const float *)p.d_aux, k, ep);
   TOMO_CUDA(cudaGetLastError());
   return TOMO_OK;
 }

@@ -52,16 +52,16 @@ __device__ __forceinline__ PdEval pd_eval(float x, float y, const PdAngle &g, fl
 // whose sub-samples can land in (b-1, b+1).
 __global__ void __launch_bounds__(128) pd_forward_kernel(
     const float *__restrict__ img, float *__restrict__ sino, const PdAngle *__restrict__ tab,
-    int n, int nh, int na) {
+    int n, int nh, int na, FwdEpi ep) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   const int v = blockIdx.y;
   const size_t z = blockIdx.z;
-  if (b >= n) return;
+  const bool live = b < n;
   const PdAngle g = tab[v];
   const float *I = img + z * (size_t)n * n;
   const float fnh = (float)nh;
   float acc = 0.0f;
-  if (b >= 1) {
+  if (live && b >= 1) {
     // T ~ nh - sigma*((y0+d) c - (x0+d) s), sigma = sign(c)
     const float sg = g.c >= 0.0f ? 1.0f : -1.0f;
     const bool by_rows = fabsf(g.s) >= fabsf(g.c);
@@ -97,7 +97,7 @@ __global__ void __launch_bounds__(128) pd_forward_kernel(
       }
     }
   }
-  sino[z * (size_t)na * n + (size_t)v * n + b] = acc;
+  fwd_store(ep, acc, live, z * (size_t)na * n + (size_t)v * n + (live ? b : 0), sino);
 }
 
 constexpr int kPdChunk = 1024;
@@ -106,7 +106,7 @@ constexpr int kPdChunk = 1024;
 // loop row is i = n-1-R.
 __global__ void __launch_bounds__(256) pd_adjoint_kernel(
     const float *__restrict__ sino, float *__restrict__ img, const PdAngle *__restrict__ tab,
-    int n, int nh, int na) {
+    int n, int nh, int na, AdjEpi ep) {
   __shared__ PdAngle stab[kPdChunk];
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   const int R = blockIdx.y * blockDim.y + threadIdx.y;
@@ -135,7 +135,7 @@ __global__ void __launch_bounds__(256) pd_adjoint_kernel(
       }
     }
   }
-  if (live) img[z * (size_t)n * n + (size_t)R * n + j] = acc;
+  adj_store(ep, acc, live, z * (size_t)n * n + (size_t)(live ? R : 0) * n + (live ? j : 0), img);
 }
 
 }  // namespace
@@ -160,18 +160,18 @@ int pd_setup(Plan &p) {
   return TOMO_OK;
 }
 
-int pd_forward(Plan &p, const float *d_img, float *d_sino, cudaStream_t s) {
+int pd_forward(Plan &p, const float *d_img, float *d_sino, cudaStream_t s, const FwdEpi &ep) {
   const int n = p.g.n, na = p.g.na, nz = p.g.nz;
   dim3 fb(128), fg((n + 127) / 128, na, nz);
-  pd_forward_kernel<<<fg, fb, 0, s>>>(d_img, d_sino, (const PdAngle *)p.d_angles, n, p.nh, na);
+  pd_forward_kernel<<<fg, fb, 0, s>>>(d_img, d_sino, (const PdAngle *)p.d_angles, n, p.nh, na, ep);
   TOMO_CUDA(cudaGetLastError());
   return TOMO_OK;
 }
 
-int pd_adjoint(Plan &p, const float *d_sino, float *d_img, cudaStream_t s) {
+int pd_adjoint(Plan &p, const float *d_sino, float *d_img, cudaStream_t s, const AdjEpi &ep) {
   const int n = p.g.n, na = p.g.na, nz = p.g.nz;
   dim3 ab(32, 8), ag((n + 31) / 32, (n + 7) / 8, nz);
-  pd_adjoint_kernel<<<ag, ab, 0, s>>>(d_sino, d_img, (const PdAngle *)p.d_angles, n, p.nh, na);
+  pd_adjoint_kernel<<<ag, ab, 0, s>>>(d_sino, d_img, (const PdAngle *)p.d_angles, n, p.nh, na, ep);
   TOMO_CUDA(cudaGetLastError());
   return TOMO_OK;
 }

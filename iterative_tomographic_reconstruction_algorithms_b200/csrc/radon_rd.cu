@@ -77,15 +77,16 @@ __device__ __forceinline__ float rd_alpha(int idx, int d, float p, float e) {
 
 __global__ void __launch_bounds__(128) rd_forward_kernel(
     const float *__restrict__ img, float *__restrict__ sino, const RdAngle *__restrict__ tab,
-    int n, int nh, int na) {
+    int n, int nh, int na, FwdEpi ep) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   const int v = blockIdx.y;
   const size_t z = blockIdx.z;
-  if (b >= n) return;
+  const bool live = b < n;
   const RdAngle g = tab[v];
   const float *I = img + z * (size_t)n * n;
   float acc = 0.0f;
-  if (g.mode == 1) {  // |s| < 1e-7: bin n-1-i <- column i, i >= 1 (radon_rd.c:96-105)
+  if (!live) {
+  } else if (g.mode == 1) {  // |s| < 1e-7: bin n-1-i <- column i, i >= 1 (radon_rd.c:96-105)
     const int i = n - 1 - b;
     if (i >= 1)
       for (int j = 0; j < n; ++j) acc += __ldg(I + (size_t)j * n + i);
@@ -125,14 +126,14 @@ __global__ void __launch_bounds__(128) rd_forward_kernel(
       }
     }
   }
-  sino[z * (size_t)na * n + (size_t)v * n + b] = acc;
+  fwd_store(ep, acc, live, z * (size_t)na * n + (size_t)v * n + (live ? b : 0), sino);
 }
 
 constexpr int kRdChunk = 256;
 
 __global__ void __launch_bounds__(128) rd_adjoint_kernel(
     const float *__restrict__ sino, float *__restrict__ img, const RdAngle *__restrict__ tab,
-    int n, int nh, int na) {
+    int n, int nh, int na, AdjEpi ep) {
   __shared__ RdAngle stab[kRdChunk];
   const int J = blockIdx.x * blockDim.x + threadIdx.x;  // column (walk y index jj + nh)
   const int I = blockIdx.y * blockDim.y + threadIdx.y;  // row    (walk x index ii + nh)
@@ -208,7 +209,7 @@ __global__ void __launch_bounds__(128) rd_adjoint_kernel(
       }
     }
   }
-  if (live) img[z * (size_t)n * n + (size_t)I * n + J] = acc;
+  adj_store(ep, acc, live, z * (size_t)n * n + (size_t)(live ? I : 0) * n + (live ? J : 0), img);
 }
 
 }  // namespace
@@ -240,18 +241,18 @@ int rd_setup(Plan &p) {
   return TOMO_OK;
 }
 
-int rd_forward(Plan &p, const float *d_img, float *d_sino, cudaStream_t s) {
+int rd_forward(Plan &p, const float *d_img, float *d_sino, cudaStream_t s, const FwdEpi &ep) {
   const int n = p.g.n, na = p.g.na, nz = p.g.nz;
   dim3 fb(128), fg((n + 127) / 128, na, nz);
-  rd_forward_kernel<<<fg, fb, 0, s>>>(d_img, d_sino, (const RdAngle *)p.d_angles, n, p.nh, na);
+  rd_forward_kernel<<<fg, fb, 0, s>>>(d_img, d_sino, (const RdAngle *)p.d_angles, n, p.nh, na, ep);
   TOMO_CUDA(cudaGetLastError());
   return TOMO_OK;
 }
 
-int rd_adjoint(Plan &p, const float *d_sino, float *d_img, cudaStream_t s) {
+int rd_adjoint(Plan &p, const float *d_sino, float *d_img, cudaStream_t s, const AdjEpi &ep) {
   const int n = p.g.n, na = p.g.na, nz = p.g.nz;
   dim3 ab(32, 4), ag((n + 31) / 32, (n + 3) / 4, nz);
-  rd_adjoint_kernel<<<ag, ab, 0, s>>>(d_sino, d_img, (const RdAngle *)p.d_angles, n, p.nh, na);
+  rd_adjoint_kernel<<<ag, ab, 0, s>>>(d_sino, d_img, (const RdAngle *)p.d_angles, n, p.nh, na, ep);
   TOMO_CUDA(cudaGetLastError());
   return TOMO_OK;
 }

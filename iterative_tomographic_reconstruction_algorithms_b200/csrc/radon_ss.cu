@@ -53,13 +53,13 @@ __global__ void ss_transpose_kernel(const float *__restrict__ in, float *__restr
 // neighbouring threads read neighbouring words.
 __global__ void __launch_bounds__(128) ss_forward_kernel(
     const float *__restrict__ img, const float *__restrict__ imgT, float *__restrict__ sino,
-    const SsAngle *__restrict__ tab, const int2 *__restrict__ lim, int n, int nh, int na) {
+    const SsAngle *__restrict__ tab, const int2 *__restrict__ lim, int n, int nh, int na, FwdEpi ep) {
   const int kt = blockIdx.x * blockDim.x + threadIdx.x;  // t + nh
   const int v = blockIdx.y;
   const size_t z = blockIdx.z;
-  if (kt >= 2 * nh) return;
+  const bool live = kt < n;  // kt == 2nh (odd n) is never reached by a ray: stays 0
   const SsAngle g = tab[v];
-  const int2 L = lim[(size_t)v * (2 * nh) + kt];
+  const int2 L = kt < 2 * nh ? lim[(size_t)v * (2 * nh) + kt] : make_int2(0, 0);
   const float ft = (float)(kt - nh);
   const float *M = (g.steep ? img : imgT) + z * (size_t)n * n;
   float acc = 0.0f;
@@ -74,7 +74,7 @@ __global__ void __launch_bounds__(128) ss_forward_kernel(
     if (q >= 0 && q <= n - 1) acc = fmaf(g.wt * w1, __ldg(row + q), acc);
     if (q + 1 >= 0 && q + 1 <= n - 1) acc = fmaf(g.wt * w, __ldg(row + q + 1), acc);
   }
-  sino[z * (size_t)na * n + (size_t)g.out_row * n + kt] = acc;
+  fwd_store(ep, acc, live, z * (size_t)na * n + (size_t)g.out_row * n + (live ? kt : 0), sino);
 }
 
 // Adjoint: one thread per output pixel, all angles in order.  For the pixel
@@ -85,7 +85,7 @@ constexpr int kSsChunk = 512;
 
 __global__ void __launch_bounds__(256) ss_adjoint_kernel(
     const float *__restrict__ sino, float *__restrict__ img, const SsAngle *__restrict__ tab,
-    const int2 *__restrict__ lim, int n, int nh, int na) {
+    const int2 *__restrict__ lim, int n, int nh, int na, AdjEpi ep) {
   __shared__ SsAngle stab[kSsChunk];
   const int C = blockIdx.x * blockDim.x + threadIdx.x;
   const int R = blockIdx.y * blockDim.y + threadIdx.y;
@@ -131,7 +131,7 @@ __global__ void __launch_bounds__(256) ss_adjoint_kernel(
       }
     }
   }
-  if (live) img[z * (size_t)n * n + (size_t)R * n + C] = acc;
+  adj_store(ep, acc, live, z * (size_t)n * n + (size_t)(live ? R : 0) * n + (live ? C : 0), img);
 }
 
 static void sort4(float *a) {
@@ -185,26 +185,22 @@ int ss_setup(Plan &p) {
   return TOMO_OK;
 }
 
-int ss_forward(Plan &p, const float *d_img, float *d_sino, cudaStream_t s) {
+int ss_forward(Plan &p, const float *d_img, float *d_sino, cudaStream_t s, const FwdEpi &ep) {
   const int n = p.g.n, na = p.g.na, nz = p.g.nz, nh = p.nh;
   dim3 tb(32, 8), tg((n + 31) / 32, (n + 31) / 32, nz);
   ss_transpose_kernel<<<tg, tb, 0, s>>>(d_img, p.d_scratch, n);
-  dim3 fb(128), fg((2 * nh + 127) / 128, na, nz);
+  dim3 fb(128), fg((n + 127) / 128, na, nz);
   ss_forward_kernel<<<fg, fb, 0, s>>>(d_img, p.d_scratch, d_sino, (const SsAngle *)p.d_angles,
-                                      (const int2 *)p.d_aux, n, nh, na);
-  if (2 * nh < n) {  // odd n: the last detector column is never written by the reference
-    TOMO_CUDA(cudaMemset2DAsync(d_sino + (n - 1), sizeof(float) * n, 0, sizeof(float),
-                                (size_t)na * nz, s));
-  }
+                                      (const int2 *)p.d_aux, n, nh, na, ep);
   TOMO_CUDA(cudaGetLastError());
   return TOMO_OK;
 }
 
-int ss_adjoint(Plan &p, const float *d_sino, float *d_img, cudaStream_t s) {
+int ss_adjoint(Plan &p, const float *d_sino, float *d_img, cudaStream_t s, const AdjEpi &ep) {
   const int n = p.g.n, na = p.g.na, nz = p.g.nz;
   dim3 ab(32, 8), ag((n + 31) / 32, (n + 7) / 8, nz);
   ss_adjoint_kernel<<<ag, ab, 0, s>>>(d_sino, d_img, (const SsAngle *)p.d_angles,
-                                      (const int2 *)p.d_aux, n, p.nh, na);
+                                      (const int2 *)p.d_aux, n, p.nh, na, ep);
   TOMO_CUDA(cudaGetLastError());
   return TOMO_OK;
 }

@@ -77,6 +77,32 @@ struct tomo_plan {
   Plan p;
 };
 
+namespace tomo {
+Plan *plan_of(tomo_plan *p) { return &p->p; }
+
+int plan_forward(Plan &p, const float *in, float *out, cudaStream_t s, const FwdEpi &ep) {
+  switch (p.g.kind) {
+    case TOMO_KIND_PD: return pd_forward(p, in, out, s, ep);
+    case TOMO_KIND_RD: return rd_forward(p, in, out, s, ep);
+    case TOMO_KIND_DD: return dd_forward(p, in, out, s, ep);
+    case TOMO_KIND_SS: return ss_forward(p, in, out, s, ep);
+    case TOMO_KIND_BSPLINE: return bs_forward(p, in, out, s, ep);
+  }
+  return fail(TOMO_EINVAL, "forward: unsupported kind");
+}
+
+int plan_adjoint(Plan &p, const float *in, float *out, cudaStream_t s, const AdjEpi &ep) {
+  switch (p.g.kind) {
+    case TOMO_KIND_PD: return pd_adjoint(p, in, out, s, ep);
+    case TOMO_KIND_RD: return rd_adjoint(p, in, out, s, ep);
+    case TOMO_KIND_DD: return dd_adjoint(p, in, out, s, ep);
+    case TOMO_KIND_SS: return ss_adjoint(p, in, out, s, ep);
+    case TOMO_KIND_BSPLINE: return bs_adjoint(p, in, out, s, ep);
+  }
+  return fail(TOMO_EINVAL, "adjoint: unsupported kind");
+}
+}  // namespace tomo
+
 extern "C" {
 
 int tomo_last_error(char *buf, size_t len) {
@@ -127,30 +153,12 @@ int tomo_plan_destroy(tomo_plan *plan) {
 
 int tomo_forward(tomo_plan *plan, const float *d_image, float *d_sino, void *stream) {
   if (!plan || !d_image || !d_sino) return fail(TOMO_EINVAL, "tomo_forward: NULL argument");
-  Plan &p = plan->p;
-  cudaStream_t s = (cudaStream_t)stream;
-  switch (p.g.kind) {
-    case TOMO_KIND_PD: return pd_forward(p, d_image, d_sino, s);
-    case TOMO_KIND_RD: return rd_forward(p, d_image, d_sino, s);
-    case TOMO_KIND_DD: return dd_forward(p, d_image, d_sino, s);
-    case TOMO_KIND_SS: return ss_forward(p, d_image, d_sino, s);
-    case TOMO_KIND_BSPLINE: return bs_forward(p, d_image, d_sino, s);
-  }
-  return fail(TOMO_EINVAL, "tomo_forward: unsupported kind");
+  return plan_forward(plan->p, d_image, d_sino, (cudaStream_t)stream, FwdEpi());
 }
 
 int tomo_adjoint(tomo_plan *plan, const float *d_sino, float *d_image, void *stream) {
   if (!plan || !d_image || !d_sino) return fail(TOMO_EINVAL, "tomo_adjoint: NULL argument");
-  Plan &p = plan->p;
-  cudaStream_t s = (cudaStream_t)stream;
-  switch (p.g.kind) {
-    case TOMO_KIND_PD: return pd_adjoint(p, d_sino, d_image, s);
-    case TOMO_KIND_RD: return rd_adjoint(p, d_sino, d_image, s);
-    case TOMO_KIND_DD: return dd_adjoint(p, d_sino, d_image, s);
-    case TOMO_KIND_SS: return ss_adjoint(p, d_sino, d_image, s);
-    case TOMO_KIND_BSPLINE: return bs_adjoint(p, d_sino, d_image, s);
-  }
-  return fail(TOMO_EINVAL, "tomo_adjoint: unsupported kind");
+  return plan_adjoint(plan->p, d_sino, d_image, (cudaStream_t)stream, AdjEpi());
 }
 
 static int ensure_host_buffers(Plan &p) {

@@ -9,6 +9,7 @@
 #include <vector>
 
 #include "../../include/tomo_b200.h"
+#include "epilogue.cuh"
 
 namespace tomo {
 
@@ -83,16 +84,20 @@ struct Plan {
   size_t d_in_bytes = 0, d_out_bytes = 0;
   cudaStream_t host_stream = nullptr;
   int device = 0;
+  // distance-driven layout (radon_dd.cu)
+  int dd_pads = 0, dd_w = 0, dd_wl = 0, dd_nR = 0, dd_nC = 0, dd_nS = 0;
 };
 
 size_t image_elems(const Plan &p);
 size_t sino_elems(const Plan &p);
 
 // One setup/forward/adjoint triple per projector kind.
-#define TOMO_DECLARE_KIND(k)                                                  \
-  int k##_setup(Plan &p);                                                     \
-  int k##_forward(Plan &p, const float *d_img, float *d_sino, cudaStream_t s); \
-  int k##_adjoint(Plan &p, const float *d_sino, float *d_img, cudaStream_t s);
+#define TOMO_DECLARE_KIND(k)                                                    \
+  int k##_setup(Plan &p);                                                       \
+  int k##_forward(Plan &p, const float *d_img, float *d_sino, cudaStream_t s,    \
+                  const FwdEpi &ep = FwdEpi());                                 \
+  int k##_adjoint(Plan &p, const float *d_sino, float *d_img, cudaStream_t s,    \
+                  const AdjEpi &ep = AdjEpi());
 TOMO_DECLARE_KIND(dd)  // radon_dd.cu
 TOMO_DECLARE_KIND(ss)  // radon_ss.cu
 TOMO_DECLARE_KIND(pd)  // radon_pd.cu
