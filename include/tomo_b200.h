@@ -179,6 +179,24 @@ int tomo_gen_backproj(const float *sino, int npix, const float *angles, int nang
                       const float *lut, int lut_size, float support_bspline,
                       float *image);
 
+/* gridrec_v4_forwproj.c:59 `void gridrec_v4_forwproj(float *S, int npix, int nang,
+ * float *angles, float *param, float *lut, float *deapod, float *I, char *fftwfn)`,
+ * bound at gridrec_v4.pyx:10-11.  Angles in degrees; param[8] = {ctr, filter,
+ * filter source, oversampling, interp (0 nearest, 1 linear), len(lut)-5, kernel
+ * width, Radon degree}; deapod is [pdim][pdim].  Like the reference it OVERWRITES
+ * S.  fftwfn (an FFTW wisdom file) is accepted and ignored. */
+int tomo_gridrec_forwproj(float *S, int npix, int nang, const float *angles, const float *param,
+                          const float *lut, const float *deapod, const float *I, const char *fftwfn);
+
+/* gridrec_v4_backproj.c:64 `void gridrec_v4_backproj(float *sino, int npix, int nang,
+ * float *angles, float *param, float *lut, float *deapod, float *filter_ext, float *rec,
+ * char *fftwfn)`, bound at gridrec_v4.pyx:7-8.  Overwrites rec.  Only the built-in
+ * filters (param[2] == 0, what the reference classes pass) are provided;
+ * filter_ext and fftwfn are accepted and ignored. */
+int tomo_gridrec_backproj(const float *sino, int npix, int nang, const float *angles,
+                          const float *param, const float *lut, const float *deapod,
+                          const float *filter_ext, float *rec, const char *fftwfn);
+
 #ifdef __cplusplus
 }
 #endif

@@ -176,7 +176,7 @@ int tomo_solver_create(tomo_plan *plan, int algo, const float *d_b, void *stream
   Plan &p = *S.p;
   cudaStream_t st = (cudaStream_t)stream;
   const size_t ni = image_elems(p), ns = sino_elems(p);
-  S.nparts = (size_t)((p.g.n + 127) / 128) * 4 * p.g.na * p.g.nz;
+  S.nparts = p.fwd_warps;
   S.cap = 1 << 16;
   int rc = TOMO_OK;
   float *ones_i = nullptr, *ones_s = nullptr;

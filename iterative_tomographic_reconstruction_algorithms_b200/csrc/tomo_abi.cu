@@ -40,6 +40,8 @@ static void release(Plan &p) {
   if (p.d_in) cudaFree(p.d_in);
   if (p.d_out) cudaFree(p.d_out);
   if (p.host_stream) cudaStreamDestroy(p.host_stream);
+  if (p.ext && p.ext_free) p.ext_free(p.ext);
+  p.ext = nullptr;
   p.d_angles = p.d_aux = nullptr;
   p.d_scratch = p.d_in = p.d_out = nullptr;
   p.host_stream = nullptr;
@@ -63,6 +65,7 @@ static int validate(const tomo_geom *g) {
     case TOMO_KIND_DD:
     case TOMO_KIND_SS:
     case TOMO_KIND_BSPLINE:
+    case TOMO_KIND_GRID:
       return TOMO_OK;
     default:
       return fail(TOMO_EINVAL, "projector kind " + std::to_string(g->kind) + " is not available");
@@ -87,6 +90,7 @@ int plan_forward(Plan &p, const float *in, float *out, cudaStream_t s, const Fwd
     case TOMO_KIND_DD: return dd_forward(p, in, out, s, ep);
     case TOMO_KIND_SS: return ss_forward(p, in, out, s, ep);
     case TOMO_KIND_BSPLINE: return bs_forward(p, in, out, s, ep);
+    case TOMO_KIND_GRID: return grid_forward(p, in, out, s, ep);
   }
   return fail(TOMO_EINVAL, "forward: unsupported kind");
 }
@@ -98,6 +102,7 @@ int plan_adjoint(Plan &p, const float *in, float *out, cudaStream_t s, const Adj
     case TOMO_KIND_DD: return dd_adjoint(p, in, out, s, ep);
     case TOMO_KIND_SS: return ss_adjoint(p, in, out, s, ep);
     case TOMO_KIND_BSPLINE: return bs_adjoint(p, in, out, s, ep);
+    case TOMO_KIND_GRID: return grid_adjoint(p, in, out, s, ep);
   }
   return fail(TOMO_EINVAL, "adjoint: unsupported kind");
 }
@@ -132,6 +137,7 @@ int tomo_plan_create(const tomo_geom *geom, tomo_plan **out) {
     case TOMO_KIND_DD: rc = dd_setup(p); break;
     case TOMO_KIND_SS: rc = ss_setup(p); break;
     case TOMO_KIND_BSPLINE: rc = bs_setup(p); break;
+    case TOMO_KIND_GRID: rc = grid_setup(p); break;
     default:
       rc = fail(TOMO_EINVAL, "unsupported kind");
   }
@@ -140,6 +146,7 @@ int tomo_plan_create(const tomo_geom *geom, tomo_plan **out) {
     delete tp;
     return rc;
   }
+  if (!p.fwd_warps) p.fwd_warps = (size_t)((p.g.n + 127) / 128) * 4 * p.g.na * p.g.nz;
   *out = tp;
   return TOMO_OK;
 }
@@ -314,4 +321,48 @@ extern "C" int tomo_gen_backproj(const float *sino, int npix, const float *angle
   if (!lut) return fail(TOMO_EINVAL, "gen_backproj: lut is NULL");
   return dropin_radon(TOMO_KIND_BSPLINE, image, npix, angles, nang, 1, const_cast<float *>(sino),
                       lut, lut_size, support_bspline);
+}
+
+// gridrec_v4.pyx:7-11 binds gridrec_v4_forwproj / gridrec_v4_backproj.  Unlike
+// the Radon kernels these reference functions OVERWRITE their output.
+namespace {
+int gridrec_call(bool forward, const float *in, float *out, int npix, int nang, const float *angles,
+                 const float *param, const float *lut, const float *deapod, int lut_len) {
+  if (!in || !out || !angles || !param || !lut || !deapod)
+    return fail(TOMO_EINVAL, "gridrec: NULL argument");
+  std::lock_guard<std::mutex> lk(g_dropin_mu);
+  tomo_geom g{};
+  g.kind = TOMO_KIND_GRID;
+  g.n = npix;
+  g.na = nang;
+  g.nz = 1;
+  g.angles = angles;
+  g.grid_param = param;
+  g.grid_lut = lut;
+  g.grid_lut_len = lut_len;
+  g.grid_deapod = deapod;
+  tomo_plan *plan = nullptr;
+  int rc = tomo_plan_create(&g, &plan);
+  if (rc) return rc;
+  rc = forward ? tomo_forward_host(plan, in, out) : tomo_adjoint_host(plan, in, out);
+  tomo_plan_destroy(plan);
+  return rc;
+}
+}  // namespace
+
+extern "C" int tomo_gridrec_forwproj(float *S, int npix, int nang, const float *angles,
+                                     const float *param, const float *lut, const float *deapod,
+                                     const float *I, const char *fftwfn) {
+  (void)fftwfn;
+  if (!param) return fail(TOMO_EINVAL, "gridrec: param is NULL");
+  return gridrec_call(true, I, S, npix, nang, angles, param, lut, deapod, (int)param[5] + 5);
+}
+
+extern "C" int tomo_gridrec_backproj(const float *sino, int npix, int nang, const float *angles,
+                                     const float *param, const float *lut, const float *deapod,
+                                     const float *filter_ext, float *rec, const char *fftwfn) {
+  (void)fftwfn;
+  (void)filter_ext;  // only read by the reference when param[2] != 0, which is rejected
+  if (!param) return fail(TOMO_EINVAL, "gridrec: param is NULL");
+  return gridrec_call(false, sino, rec, npix, nang, angles, param, lut, deapod, (int)param[5] + 5);
 }

@@ -86,6 +86,11 @@ struct Plan {
   int device = 0;
   // distance-driven layout (radon_dd.cu)
   int dd_pads = 0, dd_w = 0, dd_wl = 0, dd_nR = 0, dd_nC = 0, dd_nS = 0;
+  // warps of the forward launch that write residual partial sums (solver.cu)
+  size_t fwd_warps = 0;
+  // kind-specific state owned by the plan (gridding), freed with ext_free
+  void *ext = nullptr;
+  void (*ext_free)(void *) = nullptr;
 };
 
 size_t image_elems(const Plan &p);
@@ -103,6 +108,7 @@ TOMO_DECLARE_KIND(ss)  // radon_ss.cu
 TOMO_DECLARE_KIND(pd)  // radon_pd.cu
 TOMO_DECLARE_KIND(rd)  // radon_rd.cu
 TOMO_DECLARE_KIND(bs)  // bspline.cu
+TOMO_DECLARE_KIND(grid)  // grid.cu
 #undef TOMO_DECLARE_KIND
 
 // Plan-less pieces of the dd forward (radon_dd.cu), used by dd_noalloc.cu.

@@ -192,3 +192,32 @@ class Oracle:
         self.L.orc_bspline(_fp(data), n, _fp(a), na, _fp(lut), int(param[0]),
                            float(np.float32(param[1])), oper, _dp(out))
         return out
+
+
+def read_tiff_strip(path) -> np.ndarray:
+    """Minimal reader for the reference's uncompressed single-image TIFF data files
+    (data/*.tif): little-endian, one strip or contiguous strips, float32/float64."""
+    import struct
+    raw = Path(path).read_bytes()
+    assert raw[:2] == b"II", "big-endian TIFF not supported"
+    off = struct.unpack_from("<I", raw, 4)[0]
+    n = struct.unpack_from("<H", raw, off)[0]
+    tags = {}
+    types = {3: ("H", 2), 4: ("I", 4)}
+    for i in range(n):
+        tag, typ, cnt, val = struct.unpack_from("<HHII", raw, off + 2 + 12 * i)
+        if typ in types:
+            fmt, size = types[typ]
+            if cnt * size <= 4:
+                vals = struct.unpack_from("<" + fmt * cnt, raw, off + 2 + 12 * i + 8)
+            else:
+                vals = struct.unpack_from("<" + fmt * cnt, raw, val)
+            tags[tag] = vals
+    width, height = tags[256][0], tags[257][0]
+    bits = tags.get(258, (32,))[0]
+    fmt = tags.get(339, (3,))[0]
+    assert fmt == 3 and tags.get(259, (1,))[0] == 1, "only uncompressed IEEE float supported"
+    dtype = np.dtype("<f8") if bits == 64 else np.dtype("<f4")
+    strips, counts = tags[273], tags[279]
+    buf = b"".join(raw[o:o + c] for o, c in zip(strips, counts))
+    return np.frombuffer(buf, dtype=dtype, count=width * height).reshape(height, width).copy()

@@ -83,6 +83,35 @@ def main() -> None:
         data[f"{name}/fwd"] = R.bspline(0, img, a32, lut, param)
         data[f"{name}/adj"] = R.bspline(1, sino, a32, lut, param)
     np.savez_compressed(OUT / "bspline_golden.npz", **data)
+
+    # gridding pair: the reference's own golden pair (data/shepp_logan_pix0256.tif
+    # and its grid-PSWF sinogram data/shepp_logan_pix0256_ang0304_sino.tif, made
+    # by gridding_forward.py with its defaults: prolate kernel, W=7, os=2, nn,
+    # errs=1e-3, 304 angles on [0, 180)), plus reference outputs on seeded inputs.
+    from oracle.oracle import read_tiff_strip
+    from iterative_tomographic_reconstruction_algorithms_b200 import gridrec_lut as glut
+    ref_data = Path("/root/reference/data")
+    data = {"sl/image": read_tiff_strip(ref_data / "shepp_logan_pix0256.tif").astype(np.float32),
+            "sl/sino": read_tiff_strip(ref_data / "shepp_logan_pix0256_ang0304_sino.tif")}
+    for name, n, na, kernel, os_, interp, W, errs, rdeg, filt in [
+            ("n64_pswf_nn", 64, 90, "pswf", 2.0, "nn", 7.0, 1e-3, 0, 0),
+            ("n96_kb_lin", 96, 120, "kb", 2.0, "lin", 6.0, 6e-6, 0, 0),
+            ("n100_kb_os15", 100, 75, "kb", 1.5, "lin", 6.6, 6e-6, 0, 0),
+            ("n64_prolate_dpc", 64, 60, "prolate", 2.0, "nn", 7.0, 1e-3, 1, 0),
+            ("n80_pswf_ramp", 80, 96, "pswf", 2.0, "nn", 7.0, 1e-3, 0, 1)]:
+        Wp, lut, deapod = glut.configure_regridding(n, kernel, os_, interp, W, errs)
+        param = np.array([0.0, filt, 0, os_, 0 if interp == "nn" else 1, len(lut) - 5, Wp, rdeg], np.float32)
+        deg = np.linspace(0, 180, na, endpoint=False).astype(np.float32)
+        img = rng.standard_normal((n, n)).astype(np.float32)
+        sino = rng.standard_normal((na, n)).astype(np.float32)
+        cfg = np.array([n, na, os_, 0 if interp == "nn" else 1, W, errs, rdeg, filt], np.float64)
+        data[f"{name}/cfg"] = cfg
+        data[f"{name}/kernel"] = np.array(kernel)
+        data[f"{name}/image"] = img
+        data[f"{name}/sino"] = sino
+        data[f"{name}/fwd"] = R.gridrec(0, img, deg, param, lut.astype(np.float32), deapod.astype(np.float32))
+        data[f"{name}/adj"] = R.gridrec(1, sino, deg, param, lut.astype(np.float32), deapod.astype(np.float32))
+    np.savez_compressed(OUT / "grid_golden.npz", **data)
     print("wrote", sorted(p.name for p in OUT.glob("*.npz")))
 
 
