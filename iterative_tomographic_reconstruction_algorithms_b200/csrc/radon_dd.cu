@@ -18,10 +18,16 @@
 // q = ((i - nh) + 0.5) * k, P = x - q, D = x * r (x = j - nh, k = c*r,
 // r = 1/s or 1/c; radon_dd.c:101-115 and 196-207 under -O3 -ffast-math).
 //
-// Forward: one thread per (detector, angle, slice) walks the image lines that
-// overlap its detector and the pixels of each line inside [D_m, D_m+1].
-// Adjoint: one thread per pixel walks the angles and the (at most two)
-// detectors its interval overlaps.  Both read zero-guarded copies of their
+// Forward: the overlap-weighted sum of a line over [D_m, D_m+1] is
+// F(D_m+1) - F(D_m), F the running integral of the line, held as a double
+// prefix sum per image row and column.  One thread per (detector, angle,
+// slice) evaluates F once per line at its lower boundary and takes the upper
+// one from the neighbouring lane, whatever the detector width.  (The pixel
+// widths of the reference are P_j+1 - P_j in float, i.e. 1 to within an ulp of
+// P; the prefix sum takes them as 1, a difference of ~5e-8 relative L2.)
+// Adjoint: one thread per 2x2 pixel tile walks the angles; per angle and line
+// a segment of two pixels overlaps at most three detectors, whose boundaries
+// and values the two pixels share.  Both read zero-guarded copies of their
 // input (scratch owned by the plan), so the inner loops carry no bounds tests;
 // the exact dropped-piece rule only matters for the last pixel of a line or
 // the last detector and is evaluated on a separate path there.  No atomics:
@@ -238,128 +244,248 @@ __global__ void dd_pad_sino_kernel(const float *__restrict__ sino, float *__rest
   }
 }
 
-__global__ void __launch_bounds__(128) dd_forward_v2_kernel(
-    const float *__restrict__ Lr, const float *__restrict__ Lc, float *__restrict__ sino,
-    const DdAngle *__restrict__ tab, int n, int nh, int na, int wl, FwdEpi ep) {
-  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+// Line prefix sums in double, interleaved with the line values:
+// SL[line][kk] = {S(kk), L[kk]} for kk in [-1, n], S(kk) = sum_{j < kk} L[j],
+// with the guards SL[-1] = {0, 0} and SL[n] = {S(n), 0}.  The integral of a
+// line from its start to a boundary D inside pixel kk is then
+// F(D) = S(kk) + (D - P_kk) L[kk] for every kk in [-1, n] (pixel widths 1).
+// One block per line; passes of 256 values, each a fixed-order block scan,
+// so the sums are deterministic.
+constexpr int kScanThreads = 256;
+__global__ void __launch_bounds__(kScanThreads) dd_prefix_kernel(const float *__restrict__ L,
+                                                                 double2 *__restrict__ SL, int n, int wl,
+                                                                 int wsl) {
+  __shared__ double wsum[kScanThreads / 32];
+  __shared__ double carry_s;
+  const size_t line = blockIdx.x;
+  const float *src = L + line * wl + kPadL;
+  double2 *dst = SL + line * wsl + 1;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  double carry = 0.0;
+  for (int base = 0; base < n; base += kScanThreads) {
+    const int k = base + tid;
+    const float vf = k < n ? src[k] : 0.0f;
+    double x = (double)vf;  // inclusive warp scan
+    for (int o = 1; o < 32; o <<= 1) {
+      const double y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (lane == 31) wsum[warp] = x;
+    __syncthreads();
+    double before = carry;  // carry + totals of the earlier warps, in warp order
+    for (int w = 0; w < warp; ++w) before += wsum[w];
+    if (k < n) dst[k] = make_double2(before + (x - (double)vf), (double)vf);
+    if (tid == kScanThreads - 1) carry_s = before + x;
+    __syncthreads();
+    carry = carry_s;
+  }
+  if (tid == 0) {
+    dst[-1] = make_double2(0.0, 0.0);
+    dst[n] = make_double2(carry, 0.0);
+  }
+}
+
+// Lines i of [0, n) with q_i = ((i - nh) + 0.5) k inside [qlo, qhi], widened
+// by one line on each side; [ia, ib] is empty when ia > ib.
+__device__ __forceinline__ void dd_line_range(double qlo, double qhi, double k, int n, int nh, int &ia,
+                                              int &ib) {
+  if (k == 0.0) {
+    const bool all = qlo <= 0.0 && 0.0 <= qhi;
+    ia = all ? 0 : n;
+    ib = all ? n - 1 : -1;
+    return;
+  }
+  const double ya = qlo / k, yb = qhi / k;
+  const double flo = floor(fmin(ya, yb) + nh - 0.5) - 1.0, fhi = ceil(fmax(ya, yb) + nh - 0.5) + 1.0;
+  ia = flo < 0.0 ? 0 : (flo > (double)(n - 1) ? n : (int)flo);
+  ib = fhi > (double)(n - 1) ? n - 1 : (fhi < 0.0 ? -1 : (int)fhi);
+}
+
+// Forward.  A warp owns 31 consecutive detectors (lane 31 only supplies the
+// upper boundary of lane 30).  Lane j accumulates T_j = sum over lines of
+// F(D_j) at its lower boundary, and detector m = T_m+1 - T_m: one integral
+// evaluation per line and detector, whatever the detector's width.  The lines
+// on which the dropped last piece of the line can belong to one of the warp's
+// detectors (P_n within the warp's detector span, or beyond D_n for the warp
+// holding detector n-1) form one contiguous band; there every lane walks the
+// pieces exactly instead.
+constexpr int kFwdDet = 31;
+constexpr int kFwdWarps = 4;
+__global__ void __launch_bounds__(32 * kFwdWarps) dd_forward_v4_kernel(
+    const float *__restrict__ Lr, const float *__restrict__ Lc, const double2 *__restrict__ SLr,
+    const double2 *__restrict__ SLc, float *__restrict__ sino, const DdAngle *__restrict__ tab, int n,
+    int nh, int na, int wl, int wsl, FwdEpi ep) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int mA = (blockIdx.x * kFwdWarps + warp) * kFwdDet;
+  const int m = mA + lane;
   const int v = blockIdx.y;
   const size_t z = blockIdx.z;
-  const bool live = m < n;
+  const bool live = lane < kFwdDet && m < n;
   const DdAngle g = tab[v];
   float acc = 0.0f;
-  if (live) {
-    const float *Rz = Lr + z * (size_t)n * wl + kPadL, *Cz = Lc + z * (size_t)n * wl + kPadL;
-    if (g.mode == DD_ROWSUM) {  // detector m <- image row m = Lc[j][m]
+  const float *Rz = Lr + z * (size_t)n * wl + kPadL, *Cz = Lc + z * (size_t)n * wl + kPadL;
+  if (g.mode == DD_ROWSUM) {
+    if (live)
       for (int j = 0; j < n; ++j) acc += __ldg(Cz + (size_t)j * wl + m);
-    } else if (g.mode == DD_COLSUM) {  // detector m <- image column m = Lr[j][m]
+  } else if (g.mode == DD_COLSUM) {
+    if (live)
       for (int j = 0; j < n; ++j) acc += __ldg(Rz + (size_t)j * wl + m);
-    } else if (g.mode == DD_ROWS || g.mode == DD_COLS) {
-      const float *L = g.mode == DD_ROWS ? Rz : Cz;
-      const float r = g.r, k = g.k;
-      const float Dlo = det_bound(m, nh, r), Dhi = det_bound(m + 1, nh, r);
-      const float Dn = det_bound(n, nh, r);
-      int i0 = 0, i1 = n - 1;
-      if (k != 0.0f) {
-        const double qa = -(double)nh - (double)Dhi, qb = (double)(n - nh) - (double)Dlo;
-        const double ya = qa / (double)k, yb = qb / (double)k;
-        const double flo = floor(fmin(ya, yb) + nh - 0.5) - 1.0, fhi = ceil(fmax(ya, yb) + nh - 0.5) + 1.0;
-        i0 = flo < 0.0 ? 0 : (flo > (double)(n - 1) ? n : (int)flo);
-        i1 = fhi > (double)(n - 1) ? n - 1 : (fhi < 0.0 ? -1 : (int)fhi);
-      }
-      const float fnh = (float)nh;
-      const float lo_nh = Dlo + fnh, hi_nh = Dhi + fnh;
-      float y = (float)(i0 - nh) + 0.5f;
-      for (int i = i0; i <= i1; ++i, y += 1.0f) {
+  } else if ((g.mode == DD_ROWS || g.mode == DD_COLS) && mA < n) {
+    const float *L = g.mode == DD_ROWS ? Rz : Cz;
+    const double2 *SL = (g.mode == DD_ROWS ? SLr : SLc) + z * (size_t)n * wsl + 1;
+    const float r = g.r, k = g.k;
+    const float Dlo = det_bound(m, nh, r), Dhi = det_bound(m + 1, nh, r);
+    const float Dn = det_bound(n, nh, r);
+    const int mB = min(mA + kFwdDet - 1, n - 1);
+    const double DA = (double)det_bound(mA, nh, r), DB = (double)det_bound(mB + 1, nh, r);
+    const double kd = (double)k, PN = (double)(n - nh);
+    int i0, i1, j0, j1;
+    dd_line_range(-(double)nh - DB, PN - DA, kd, n, nh, i0, i1);
+    const double margin = 2.0 + 1e-6 * (fabs(DA) + fabs(DB) + (double)n * (1.0 + fabs(kd)));
+    const double BL = DA - margin, BH = mB == n - 1 ? 1e30 : DB + margin;
+    dd_line_range(PN - BH, PN - BL, kd, n, nh, j0, j1);
+    j0 = max(j0, i0);
+    j1 = min(j1, i1);
+    if (j0 > j1) {  // no band: all lines are fast
+      j0 = i1 + 1;
+      j1 = i1;
+    }
+    const float lo_nh = __fadd_rn(Dlo, (float)nh);
+    double T = 0.0, X = 0.0;
+    for (int seg = 0; seg < 2; ++seg) {
+      const int ia = seg == 0 ? i0 : j1 + 1, ib = seg == 0 ? j0 : i1 + 1;
+      float y = (float)(ia - nh) + 0.5f;
+      const double2 *sl = SL + (size_t)ia * wsl;
+#pragma unroll 4
+      for (int i = ia; i < ib; ++i) {
         const float q = __fmul_rn(y, k);
-        const float *row = L + (size_t)i * wl;
-        const int kk1 = (int)floorf(hi_nh + q);
-        if (kk1 >= n - 2 || m == n - 1) {  // the line's dropped piece may be ours
-          acc += dd_fwd_line_exact(row, m, q, r, Dlo, Dhi, Dn, n, nh);
-          continue;
-        }
-        int kk = max((int)floorf(lo_nh + q), -1);
-        float P = pix_bound(kk, nh, q);
-        if (P > Dlo && kk > -1) {  // rounding put the estimate one pixel too far
-          --kk;
-          P = pix_bound(kk, nh, q);
-        }
-        for (; P < Dhi && kk <= n; ++kk) {
-          const float P1 = pix_bound(kk + 1, nh, q);
-          const float w = fmaxf(__fsub_rn(fminf(P1, Dhi), fmaxf(P, Dlo)), 0.0f);
-          acc = fmaf(w, __ldg(row + kk), acc);  // row[-1], row[n]: zero guards
-          P = P1;
-        }
+        const int kk = min(max(__float2int_rd(__fadd_rn(lo_nh, q)), -1), n);
+        const float Pk = __fsub_rn((float)(kk - nh), q);
+        const double2 e = __ldg(sl + kk);
+        T = fma((double)__fsub_rn(Dlo, Pk), e.y, T + e.x);
+        y = __fadd_rn(y, 1.0f);
+        sl += wsl;
       }
     }
+    if (live) {
+      float y = (float)(j0 - nh) + 0.5f;
+      for (int i = j0; i <= j1; ++i, y = __fadd_rn(y, 1.0f))
+        X += (double)dd_fwd_line_exact(L + (size_t)i * wl, m, __fmul_rn(y, k), r, Dlo, Dhi, Dn, n, nh);
+    }
+    const double Tup = __shfl_down_sync(0xffffffffu, T, 1);
+    acc = (float)((Tup - T) + X);
   }
   fwd_store(ep, acc, live, z * (size_t)na * n + (size_t)g.out_row * n + (live ? m : 0), sino);
 }
 
 constexpr int kAdjChunk = 1024;
 
-// Adjoint tables: lines = rows (ROWS) or columns (COLS); entry = {r, k, rinv, row offset}.
-__global__ void __launch_bounds__(256) dd_adjoint_v2_kernel(
+// One line segment of two pixels [P0, P1], [P1, P2] (the line's offset q is
+// applied); adds their weights times the detector values into a0, a1.  Exact
+// unless the segment touches the last pixel or detector, where the caller
+// takes dd_adj_pixel_exact instead.
+__device__ __forceinline__ void dd_adj_segment(float P0, float P1, float P2, const float4 e,
+                                               const float *__restrict__ S, float nhp, int pads, int n,
+                                               float &a0, float &a1, bool &edge) {
+  const float r = e.x;
+  int mp = (int)floorf(fmaf(P0, e.z, nhp));
+  float fm = __fsub_rn((float)mp, nhp);
+  float Dm = __fmul_rn(fm, r);
+  if (Dm > P0) {
+    --mp;
+    fm = __fsub_rn(fm, 1.0f);
+    Dm = __fmul_rn(fm, r);
+  }
+  float D1 = __fmul_rn(__fadd_rn(fm, 1.0f), r);
+  if (D1 <= P0) {
+    ++mp;
+    fm = __fadd_rn(fm, 1.0f);
+    D1 = __fmul_rn(__fadd_rn(fm, 1.0f), r);
+  }
+  edge = (unsigned)(mp - pads - (n - 3)) <= 2u;  // the segment meets detector n-1
+  const float D2 = __fmul_rn(__fadd_rn(fm, 2.0f), r);
+  const float *sp = S + __float_as_int(e.w) + mp;
+  const float v0 = __ldg(sp), v1 = __ldg(sp + 1), v2 = __ldg(sp + 2);
+  const float t0 = fminf(D1, P1);
+  a0 = fmaf(__fsub_rn(t0, P0), v0, a0);
+  a0 = fmaf(__fsub_rn(P1, t0), v1, a0);
+  const bool c = P1 >= D1;
+  const float Da = c ? D2 : D1, va = c ? v1 : v0, vb = c ? v2 : v1;
+  const float t1 = fminf(Da, P2);
+  a1 = fmaf(__fsub_rn(t1, P1), va, a1);
+  a1 = fmaf(__fsub_rn(P2, t1), vb, a1);
+}
+
+// Adjoint: one thread per 2x2 pixel tile (rows a0, a0+1; columns b0, b0+1).
+// For a ROWS angle the tile is two row segments of two pixels, for a COLS
+// angle two column segments; each segment shares its boundary and detector
+// arithmetic between its two pixels.
+__global__ void __launch_bounds__(256) dd_adjoint_v3_kernel(
     const float *__restrict__ Sp, float *__restrict__ img, const float4 *__restrict__ tabR, int nR,
     const float4 *__restrict__ tabC, int nC, const int2 *__restrict__ tabS, int nS, int n, int nh,
     int na, int w, int pads, AdjEpi ep) {
   __shared__ float4 st[kAdjChunk];
-  const int b = blockIdx.x * blockDim.x + threadIdx.x;
-  const int a = blockIdx.y * blockDim.y + threadIdx.y;
+  const int b0 = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
+  const int a0 = 2 * (blockIdx.y * blockDim.y + threadIdx.y);
   const size_t z = blockIdx.z;
-  const bool live = a < n && b < n;
+  const bool any = a0 < n && b0 < n;
   const float *S = Sp + z * (size_t)na * w;
   const int tid = threadIdx.y * blockDim.x + threadIdx.x, nthr = blockDim.x * blockDim.y;
   const float nhp = (float)(nh + pads);
-  float acc = 0.0f;
+  float acc[2][2] = {{0.f, 0.f}, {0.f, 0.f}};  // [row - a0][col - b0]
   for (int pass = 0; pass < 2; ++pass) {
     const float4 *tab = pass == 0 ? tabR : tabC;
     const int cnt_all = pass == 0 ? nR : nC;
-    // ROWS: the pixel is kk = b of line a; COLS: kk = a of line b
-    const int line = pass == 0 ? a : b, kk = pass == 0 ? b : a;
-    const float y = (float)(line - nh) + 0.5f;
-    const float xk = (float)(kk - nh), xk1 = (float)(kk + 1 - nh);
-    const bool edge_pixel = kk == n - 1;
+    // ROWS: lines are rows a0, a0+1 and the segment is columns b0, b0+1; COLS: transposed
+    const int l0 = pass == 0 ? a0 : b0, k0 = pass == 0 ? b0 : a0;
+    const float y0 = (float)(l0 - nh) + 0.5f, y1 = __fadd_rn(y0, 1.0f);
+    const float x0 = (float)(k0 - nh), x1 = __fadd_rn(x0, 1.0f), x2 = __fadd_rn(x0, 2.0f);
+    const bool edge_pixel = k0 + 1 >= n - 1;
     for (int v0 = 0; v0 < cnt_all; v0 += kAdjChunk) {
       const int cnt = min(kAdjChunk, cnt_all - v0);
       __syncthreads();
       for (int t = tid; t < cnt; t += nthr) st[t] = tab[v0 + t];
       __syncthreads();
-      if (!live) continue;
-#pragma unroll 2
+      if (!any) continue;
       for (int u = 0; u < cnt; ++u) {
         const float4 e = st[u];
-        const float r = e.x, k = e.y;
-        const int off = __float_as_int(e.w);
-        const float q = __fmul_rn(y, k);
-        const float Pk = __fsub_rn(xk, q), Pk1 = __fsub_rn(xk1, q);
-        int mp = (int)floorf(fmaf(Pk, e.z, nhp));
-        float fm = __fsub_rn((float)mp, nhp);  // m - nh, exact
-        float Dm = __fmul_rn(fm, r);
-        if (Dm > Pk) {
-          --mp;
-          fm = __fsub_rn(fm, 1.0f);
-          Dm = __fmul_rn(fm, r);
-        }
-        const float Dm1 = __fmul_rn(__fadd_rn(fm, 1.0f), r);
-        const float *srow = S + off;
-        if (edge_pixel || mp - pads >= n - 2) {
-          acc += dd_adj_pixel_exact(srow + pads, kk, q, r, n, nh);
-        } else {
-          const float w1 = fmaxf(__fsub_rn(fminf(Pk1, Dm1), fmaxf(Pk, Dm)), 0.0f);
-          const float w2 = fmaxf(__fsub_rn(Pk1, fmaxf(Dm1, Pk)), 0.0f);
-          acc = fmaf(w1, __ldg(srow + mp), acc);
-          acc = fmaf(w2, __ldg(srow + mp + 1), acc);
+        for (int li = 0; li < 2; ++li) {
+          if (l0 + li >= n) break;  // odd n: the tile's second line is outside the image
+          const float q = __fmul_rn(li ? y1 : y0, e.y);
+          const float P0 = __fsub_rn(x0, q), P1 = __fsub_rn(x1, q), P2 = __fsub_rn(x2, q);
+          float s0 = 0.0f, s1 = 0.0f;
+          bool edge;
+          dd_adj_segment(P0, P1, P2, e, S, nhp, pads, n, s0, s1, edge);
+          if (edge || edge_pixel) {
+            const float *srow = S + __float_as_int(e.w) + pads;
+            s0 = dd_adj_pixel_exact(srow, k0, q, e.x, n, nh);
+            s1 = k0 + 1 < n ? dd_adj_pixel_exact(srow, k0 + 1, q, e.x, n, nh) : 0.0f;
+          }
+          if (pass == 0) {
+            acc[li][0] += s0;
+            acc[li][1] += s1;
+          } else {
+            acc[0][li] += s0;
+            acc[1][li] += s1;
+          }
         }
       }
     }
   }
-  if (live) {
+  if (any) {
     for (int t = 0; t < nS; ++t) {  // row / column sums (|sin| or |cos| < 1e-7)
       const int2 e = __ldg(tabS + t);
-      acc += __ldg(S + e.y + pads + (e.x == DD_ROWSUM ? a : b));
+      const float *srow = S + e.y + pads;
+      for (int dr = 0; dr < 2; ++dr)
+        for (int dc = 0; dc < 2; ++dc) acc[dr][dc] += __ldg(srow + (e.x == DD_ROWSUM ? a0 + dr : b0 + dc));
     }
   }
-  adj_store(ep, acc, live, z * (size_t)n * n + (size_t)(live ? a : 0) * n + (live ? b : 0), img);
+  for (int dr = 0; dr < 2; ++dr)
+    for (int dc = 0; dc < 2; ++dc) {
+      const int a = a0 + dr, b = b0 + dc;
+      const bool live = a < n && b < n;
+      adj_store(ep, acc[dr][dc], live, z * (size_t)n * n + (size_t)(live ? a : 0) * n + (live ? b : 0), img);
+    }
 }
 
 }  // namespace
@@ -452,19 +578,34 @@ int dd_setup(Plan &p) {
     TOMO_CUDA(cudaMemcpy(aux + sizeof(float4) * (rows.size() + cols.size()), sums.data(),
                          sizeof(int2) * sums.size(), cudaMemcpyHostToDevice));
   const size_t lines = 2 * (size_t)nz * n * p.dd_wl, sp = (size_t)nz * na * p.dd_w;
-  p.scratch_bytes = sizeof(float) * (lines + sp);
+  const size_t nsum = 2 * (size_t)nz * n * (n + 2);  // double2
+  p.scratch_bytes = (sizeof(float) * (lines + sp) + 255) / 256 * 256 + sizeof(double2) * nsum;
+  // residual partials: one per warp of the forward grid (dd_forward)
+  const int per_block = kFwdDet * kFwdWarps;
+  p.fwd_warps = (size_t)((n + per_block - 1) / per_block) * kFwdWarps * na * nz;
   TOMO_CUDA(cudaMalloc(&p.d_scratch, p.scratch_bytes));
   return TOMO_OK;
 }
 
+// scratch layout: Lr | Lc (floats, nz*n*wl each) | Sp (floats) | SLr | SLc (double2, nz*n*(n+2) each)
+static double2 *dd_sums(Plan &p) {
+  const size_t fl = 2 * (size_t)p.g.nz * p.g.n * p.dd_wl + (size_t)p.g.nz * p.g.na * p.dd_w;
+  const size_t off = (fl * sizeof(float) + 255) / 256 * 256;
+  return (double2 *)((char *)p.d_scratch + off);
+}
+
 int dd_forward(Plan &p, const float *d_img, float *d_sino, cudaStream_t s, const FwdEpi &ep) {
-  const int n = p.g.n, na = p.g.na, nz = p.g.nz;
+  const int n = p.g.n, na = p.g.na, nz = p.g.nz, wsl = n + 2;
   float *Lr = p.d_scratch, *Lc = p.d_scratch + (size_t)nz * n * p.dd_wl;
+  double2 *SLr = dd_sums(p), *SLc = SLr + (size_t)nz * n * wsl;
   dim3 tb(32, 8), tg((n + 31) / 32, (n + 31) / 32, nz);
   dd_pad_image_kernel<<<tg, tb, 0, s>>>(d_img, Lr, Lc, n, p.dd_wl);
-  dim3 fb(128), fg((n + 127) / 128, na, nz);
-  dd_forward_v2_kernel<<<fg, fb, 0, s>>>(Lr, Lc, d_sino, (const DdAngle *)p.d_angles, n, p.nh, na,
-                                         p.dd_wl, ep);
+  dd_prefix_kernel<<<nz * n, kScanThreads, 0, s>>>(Lr, SLr, n, p.dd_wl, wsl);
+  dd_prefix_kernel<<<nz * n, kScanThreads, 0, s>>>(Lc, SLc, n, p.dd_wl, wsl);
+  const int per_block = kFwdDet * kFwdWarps;
+  dim3 fb(32 * kFwdWarps), fg((n + per_block - 1) / per_block, na, nz);
+  dd_forward_v4_kernel<<<fg, fb, 0, s>>>(Lr, Lc, SLr, SLc, d_sino, (const DdAngle *)p.d_angles, n, p.nh, na,
+                                         p.dd_wl, wsl, ep);
   TOMO_CUDA(cudaGetLastError());
   return TOMO_OK;
 }
@@ -477,8 +618,8 @@ int dd_adjoint(Plan &p, const float *d_sino, float *d_img, cudaStream_t s, const
                                        p.dd_pads);
   const float4 *tR = (const float4 *)p.d_aux, *tC = tR + p.dd_nR;
   const int2 *tS = (const int2 *)(tC + p.dd_nC);
-  dim3 ab(32, 8), ag((n + 31) / 32, (n + 7) / 8, nz);
-  dd_adjoint_v2_kernel<<<ag, ab, 0, s>>>(Sp, d_img, tR, p.dd_nR, tC, p.dd_nC, tS, p.dd_nS, n, p.nh,
+  dim3 ab(32, 8), ag((n + 63) / 64, (n + 15) / 16, nz);
+  dd_adjoint_v3_kernel<<<ag, ab, 0, s>>>(Sp, d_img, tR, p.dd_nR, tC, p.dd_nC, tS, p.dd_nS, n, p.nh,
                                          na, p.dd_w, p.dd_pads, ep);
   TOMO_CUDA(cudaGetLastError());
   return TOMO_OK;
