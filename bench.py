@@ -284,8 +284,10 @@ def main():
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": WORKLOAD, "slices_per_rank_per_step": 1,
                        "l2": "flushed between steps (256 MiB write)", "parallelism": f"slices x{world}"},
-            "gpu_launches": 3 * args.steps,
-            "kernel_ms": {"dd_forward(+transpose)": fwd_ms, "dd_adjoint": adj_ms},
+            "gpu_launches": 5 * args.steps,
+            "kernel_ms": {"dd_forward (line prefix sums + persistent forward)": fwd_ms,
+                          "dd_adjoint (sinogram prefix sums + persistent adjoint)": adj_ms},
+            "tuning": _lib.plan_tuning(tp.plan(1, dev.index if hasattr(dev, "index") else 0)),
             "roofline": roofline,
             "roofline_hbm": {"bound": "hbm", "achieved": hbm_bytes / (dom_ms * 1e-3) / 1e9,
                              "peak": hbm_peak, "unit": "GB/s",

@@ -91,6 +91,25 @@ int tomo_measure_onchip_peaks(double *smem_gbs, double *l1_gbs, double *fp32_tfl
 int tomo_plan_create(const tomo_geom *geom, tomo_plan **plan);
 int tomo_plan_destroy(tomo_plan *plan);
 
+/* Batched plan over `count` distance-driven geometries of different sizes
+ * (each geoms[i].kind == TOMO_KIND_DD, with its own n, na, angles and nz
+ * slices).  No reference counterpart: the reference runs independent slices
+ * in a process pool (art.py:289, sir.py:260).  Images and sinograms are packed
+ * back to back in geometry order, slice after slice, each slice C-order; the
+ * plan is then used with tomo_forward / tomo_adjoint / tomo_solver_* on those
+ * packed arrays.  Every forward or adjoint is one persistent launch over all
+ * instances (plus its prefix-sum pre-pass); results equal the per-geometry
+ * plans' bit for bit. */
+int tomo_plan_create_batch(const tomo_geom *geoms, int count, tomo_plan **plan);
+/* Number of instances (slices) of a plan and, if the arrays are given
+ * (cap >= instances + 1 entries), the offset in floats of each instance's
+ * image and sinogram in the packed arrays; entry [instances] is the total. */
+int tomo_plan_layout(tomo_plan *plan, int *instances, size_t *img_off, size_t *sino_off, size_t cap);
+/* The launch shape the plan uses (for dd: warps per block of the persistent
+ * kernels, chosen at plan creation by timing the candidates on the plan's own
+ * scratch when the workload is large enough), as text. */
+int tomo_plan_tuning(tomo_plan *plan, char *buf, size_t len);
+
 /* Forward A: d_image [nz][n][n] -> d_sino [nz][na][n] (overwritten). */
 int tomo_forward(tomo_plan *plan, const float *d_image, float *d_sino, void *stream);
 /* Adjoint A^T: d_sino [nz][na][n] -> d_image [nz][n][n] (overwritten). */

@@ -78,6 +78,10 @@ def _load() -> ctypes.CDLL:
     lib.tomo_gen_forwproj.argtypes = [_f32p, i, _f32p, i, _f32p, i, f, i, _f32p]
     lib.tomo_gen_backproj.argtypes = [_f32p, i, _f32p, i, _f32p, i, f, _f32p]
     lib.tomo_measure_onchip_peaks.argtypes = [ctypes.POINTER(ctypes.c_double)] * 3
+    lib.tomo_plan_create_batch.argtypes = [ctypes.POINTER(TomoGeom), i, ctypes.POINTER(vp)]
+    lib.tomo_plan_layout.argtypes = [vp, ctypes.POINTER(i), ctypes.POINTER(ctypes.c_size_t),
+                                     ctypes.POINTER(ctypes.c_size_t), ctypes.c_size_t]
+    lib.tomo_plan_tuning.argtypes = [vp, ctypes.c_char_p, ctypes.c_size_t]
     return lib
 
 
@@ -181,3 +185,85 @@ class Plan:
 
     def adjoint(self, y):
         return self._run(y, False)
+
+
+class BatchPlan(Plan):
+    """Distance-driven plan over geometries of different sizes (``tomo_plan_create_batch``).
+
+    ``geoms`` is a list of ``(n, angles_c)`` or ``(n, angles_c, nz)``.  Images
+    and sinograms are packed back to back in that order (each slice C-order)
+    into flat float32 arrays of ``img_total`` / ``sino_total`` elements;
+    ``img_off`` / ``sino_off`` give each instance's start.  All instances run
+    in one persistent launch per forward or adjoint.
+    """
+
+    def __init__(self, geoms):
+        self.kind = KIND_DD
+        self._keep = []
+        arr = (TomoGeom * len(geoms))()
+        for g, spec in zip(arr, geoms):
+            n, ang = int(spec[0]), np.ascontiguousarray(spec[1], dtype=np.float32)
+            self._keep.append(ang)
+            g.kind, g.n, g.na = KIND_DD, n, len(ang)
+            g.nz = int(spec[2]) if len(spec) > 2 else 1
+            g.angles = ang.ctypes.data_as(_f32p)
+        self._lock = threading.Lock()
+        h = ctypes.c_void_p()
+        check(lib.tomo_plan_create_batch(arr, len(geoms), ctypes.byref(h)), "tomo_plan_create_batch")
+        self._h = h
+        cnt = ctypes.c_int()
+        check(lib.tomo_plan_layout(h, ctypes.byref(cnt), None, None, 0), "tomo_plan_layout")
+        io = (ctypes.c_size_t * (cnt.value + 1))()
+        so = (ctypes.c_size_t * (cnt.value + 1))()
+        check(lib.tomo_plan_layout(h, None, io, so, cnt.value + 1), "tomo_plan_layout")
+        self.instances = cnt.value
+        self.img_off = np.array(io[:], dtype=np.int64)
+        self.sino_off = np.array(so[:], dtype=np.int64)
+        self.img_total, self.sino_total = int(self.img_off[-1]), int(self.sino_off[-1])
+        self.n = self.na = self.nz = 0
+        self._geoms = [(int(sp[0]), len(sp[1]), int(sp[2]) if len(sp) > 2 else 1) for sp in geoms]
+
+    def pack(self, arrays, which: str = "img"):
+        """Concatenate per-instance images (``which='img'``) or sinograms into the packed layout."""
+        shapes = _batch_shapes(self, which)
+        if len(arrays) != len(shapes):
+            raise ValueError(f"expected {len(shapes)} arrays, got {len(arrays)}")
+        for a, sh in zip(arrays, shapes):
+            if tuple(a.shape) != sh:
+                raise ValueError(f"expected shape {sh}, got {tuple(a.shape)}")
+        if isinstance(arrays[0], np.ndarray):
+            return np.concatenate([np.asarray(a, np.float32).ravel() for a in arrays])
+        torch = _torch()
+        return torch.cat([a.reshape(-1) for a in arrays])
+
+    def unpack(self, flat, which: str = "img"):
+        """Split a packed image or sinogram array into per-instance views."""
+        off = self.img_off if which == "img" else self.sino_off
+        shapes = _batch_shapes(self, which)
+        return [flat[int(off[i]):int(off[i + 1])].reshape(sh) for i, sh in enumerate(shapes)]
+
+    @property
+    def image_shape(self):
+        return (self.img_total,)
+
+    @property
+    def sino_shape(self):
+        return (self.sino_total,)
+
+    def tuning(self) -> str:
+        return plan_tuning(self)
+
+
+def plan_tuning(plan: Plan) -> str:
+    """The launch shape the plan chose (``tomo_plan_tuning``)."""
+    buf = ctypes.create_string_buffer(512)
+    check(lib.tomo_plan_tuning(plan._h, buf, len(buf)), "tomo_plan_tuning")
+    return buf.value.decode()
+
+
+def _batch_shapes(plan: BatchPlan, which: str):
+    out = []
+    for g in plan._geoms:
+        n, na, nz = g
+        out += [(n, n) if which == "img" else (na, n)] * nz
+    return out

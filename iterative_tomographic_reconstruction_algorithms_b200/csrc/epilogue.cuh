@@ -60,28 +60,35 @@ __device__ __forceinline__ size_t global_warp_slot() {
   return block * ((blockDim.x * blockDim.y * blockDim.z) / 32) + tid / 32;
 }
 
+// The forward epilogue of sinogram element e; adds (acc - b[e])^2 to r2 when
+// residuals are requested.
+__device__ __forceinline__ float fwd_apply(const FwdEpi &ep, float acc, size_t e, double &r2) {
+  if (ep.op == EPI_NONE) return acc;
+  const float bv = __ldg(ep.b + e);
+  float o;
+  if (ep.op == EPI_SIRT) o = __fmul_rn(__ldg(ep.w + e), __fsub_rn(bv, acc));
+  else if (ep.op == EPI_MLEM) o = __fdiv_rn(bv, acc == 0.0f ? kSpacing32 : acc);
+  else o = __fmul_rn(__fsub_rn(acc, bv), __ldg(ep.w + e));
+  if (ep.resid) {
+    const double d = (double)acc - (double)bv;
+    r2 += d * d;
+  }
+  return o;
+}
+
+// Warp sum of the lanes' r2 into partial-sum slot `slot` (every lane calls).
+__device__ __forceinline__ void fwd_resid_commit(const FwdEpi &ep, double r2, size_t slot) {
+  if (!ep.resid) return;
+  for (int off = 16; off; off >>= 1) r2 += __shfl_down_sync(0xffffffffu, r2, off);
+  if ((threadIdx.x & 31) == 0) ep.resid[slot] = r2;
+}
+
 // Every lane of the warp must call this (pass live = false for idle lanes).
 __device__ __forceinline__ void fwd_store(const FwdEpi &ep, float acc, bool live, size_t e,
                                           float *out) {
   double r2 = 0.0;
-  if (live) {
-    float o = acc;
-    if (ep.op != EPI_NONE) {
-      const float bv = __ldg(ep.b + e);
-      if (ep.op == EPI_SIRT) o = __fmul_rn(__ldg(ep.w + e), __fsub_rn(bv, acc));
-      else if (ep.op == EPI_MLEM) o = __fdiv_rn(bv, acc == 0.0f ? kSpacing32 : acc);
-      else o = __fmul_rn(__fsub_rn(acc, bv), __ldg(ep.w + e));
-      if (ep.resid) {
-        const double d = (double)acc - (double)bv;
-        r2 = d * d;
-      }
-    }
-    out[e] = o;
-  }
-  if (ep.resid) {
-    for (int off = 16; off; off >>= 1) r2 += __shfl_down_sync(0xffffffffu, r2, off);
-    if ((threadIdx.x & 31) == 0) ep.resid[global_warp_slot()] = r2;
-  }
+  if (live) out[e] = fwd_apply(ep, acc, e, r2);
+  fwd_resid_commit(ep, r2, global_warp_slot());
 }
 
 // Every lane of the warp must call this (pass live = false for idle lanes).

@@ -8,36 +8,47 @@
 // walks the merged list (:125-189), crediting every gap between consecutive
 // boundaries -- an overlap of pixel k with detector m -- with weight
 // |gap| * value.  Two properties of that walk are kept here:
-//   * the first gap after a label change is outside one of the two ranges and
-//     is not credited; gaps are credited only once both ranges have started;
+//   * gaps are credited only inside both ranges ([P_0, P_n] and [D_0, D_n]);
 //   * the walk stops at the first boundary whose index is n (:176-177), so the
 //     LAST overlap piece of each line (the gap ending at min(P_n, D_n)) is
 //     never credited.
-// Rather than sorting, the kernels enumerate the overlaps in closed form.
 // Every boundary is the same float the compiled reference computes:
 // q = ((i - nh) + 0.5) * k, P = x - q, D = x * r (x = j - nh, k = c*r,
 // r = 1/s or 1/c; radon_dd.c:101-115 and 196-207 under -O3 -ffast-math).
 //
-// Forward: the overlap-weighted sum of a line over [D_m, D_m+1] is
-// F(D_m+1) - F(D_m), F the running integral of the line, held as a double
-// prefix sum per image row and column.  One thread per (detector, angle,
-// slice) evaluates F once per line at its lower boundary and takes the upper
-// one from the neighbouring lane, whatever the detector width.  (The pixel
-// widths of the reference are P_j+1 - P_j in float, i.e. 1 to within an ulp of
-// P; the prefix sum takes them as 1, a difference of ~5e-8 relative L2.)
-// Adjoint: one thread per 2x2 pixel tile walks the angles; per angle and line
-// a segment of two pixels overlaps at most three detectors, whose boundaries
-// and values the two pixels share.  Both read zero-guarded copies of their
-// input (scratch owned by the plan), so the inner loops carry no bounds tests;
-// the exact dropped-piece rule only matters for the last pixel of a line or
-// the last detector and is evaluated on a separate path there.  No atomics:
-// each output element is owned by one thread, so results are deterministic.
-// The projection arithmetic of the solvers (epilogue.cuh) is applied where the
-// result is stored.
+// Rather than sorting, the overlaps are enumerated in closed form:
+//   forward  detector m of a line = F(D_m+1) - F(D_m), F the running integral
+//            of the line's pixel values, kept per image row and column as a
+//            double prefix sum (the integral-image form of distance-driven
+//            projection: Basu & De Man, "Branchless distance driven projection
+//            and backprojection", SPIE 6065, 2006).  One table read per
+//            detector and line, however wide the detector (r = 1/|s| can be
+//            large).  Pixel widths are taken as 1; the reference's are
+//            P_j+1 - P_j in float, i.e. 1 to within an ulp of P.
+//   adjoint  a pixel is at most one detector wide (r >= 1), so it overlaps the
+//            detector holding its left boundary and possibly the next: two
+//            float gaps, as the reference forms them, from one table entry
+//            {D_a, S_a, D_a+1, S_a+1} per angle.
+// The dropped last piece is subtracted where it falls (dd_dropped_piece).
+//
+// Work is described by a table of instances (one per slice, or per geometry
+// of an uneven batch) and consumed by persistent kernels: each warp takes the
+// next work item (forward: 127 detectors of one angle; adjoint: a 32x16 pixel
+// tile over all angles) from a device counter, finds its instance by binary
+// search and runs it.  Every output element is owned by one lane and its sum
+// order is fixed, so results do not depend on scheduling and are
+// deterministic.  Warps per block are chosen per plan by timing the
+// candidates (dd_autotune).  The projection arithmetic of the solvers
+// (epilogue.cuh) is applied where the result is stored.
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <tuple>
+#include <vector>
 
 #include "epilogue.cuh"
 #include "tomo_internal.cuh"
@@ -46,7 +57,6 @@ namespace tomo {
 namespace {
 
 constexpr double kPi = 3.141592653589793;
-constexpr int kPadL = 4;  // zero guard on each side of an image line copy
 
 __device__ __forceinline__ float pix_bound(int j, int nh, float q) {
   return __fsub_rn((float)(j - nh), q);
@@ -133,156 +143,74 @@ __global__ void __launch_bounds__(128) dd_forward_kernel(
   sino[z * (size_t)na * n + (size_t)g.out_row * n + m] = acc;
 }
 
-// ---------------------------------------------------------------------------
-// Exact single-line / single-pixel contributions (used on the edge paths).
-// ---------------------------------------------------------------------------
-// Detector m, line with offset q: every overlap piece, minus the dropped one.
-__device__ float dd_fwd_line_exact(const float *row, int m, float q, float r, float Dlo, float Dhi,
-                                   float Dn, int n, int nh) {
-  const float Pn = pix_bound(n, nh, q);
-  const bool lastIsPixel = Pn <= Dn;
-  int kk = (int)floorf(Dlo + q + (float)nh) - 1;
-  kk = kk < 0 ? 0 : (kk > n - 1 ? n - 1 : kk);
-  float Pk = pix_bound(kk, nh, q);
-  while (kk > 0 && Pk > Dlo) {
-    --kk;
-    Pk = pix_bound(kk, nh, q);
-  }
-  float acc = 0.0f;
-  for (; kk < n && Pk < Dhi; ++kk) {
-    const float Pk1 = pix_bound(kk + 1, nh, q);
-    const float lo = fmaxf(Pk, Dlo), hi = fminf(Pk1, Dhi);
-    if (hi > lo) {
-      const bool drop = lastIsPixel ? (kk == n - 1 && Pn <= Dhi) : (m == n - 1 && Pk1 > Dn);
-      if (!drop) acc = fmaf(__fsub_rn(hi, lo), __ldg(row + kk), acc);
-    }
-    Pk = Pk1;
-  }
-  return acc;
-}
-
-// Pixel kk of a line with offset q: every overlap piece with detectors
-// 0..n-1, minus the line's dropped piece.  srow[m] is the detector value.
-__device__ float dd_adj_pixel_exact(const float *srow, int kk, float q, float r, int n, int nh) {
-  const float Pk = pix_bound(kk, nh, q), Pk1 = pix_bound(kk + 1, nh, q);
-  const float Pn = pix_bound(n, nh, q), Dn = det_bound(n, nh, r);
-  const bool lastIsPixel = Pn <= Dn;
-  int m = (int)floorf(Pk / r + (float)nh);
-  m = m < 0 ? 0 : (m > n - 1 ? n - 1 : m);
-  float Dm = det_bound(m, nh, r);
-  while (m > 0 && Dm > Pk) {
-    --m;
-    Dm = det_bound(m, nh, r);
-  }
-  float Dm1 = det_bound(m + 1, nh, r);
-  while (m < n - 1 && Dm1 <= Pk) {
-    ++m;
-    Dm = Dm1;
-    Dm1 = det_bound(m + 1, nh, r);
-  }
-  float acc = 0.0f;
-  for (; m < n && Dm < Pk1; ++m) {
-    const float lo = fmaxf(Pk, Dm), hi = fminf(Pk1, Dm1);
-    if (hi > lo) {
-      const bool drop = lastIsPixel ? (kk == n - 1 && Pn <= Dm1) : (m == n - 1 && Pk1 > Dn);
-      if (!drop) acc = fmaf(__fsub_rn(hi, lo), __ldg(srow + m), acc);
-    }
-    Dm = Dm1;
-    Dm1 = det_bound(m + 2, nh, r);
-  }
-  return acc;
-}
 
 // ---------------------------------------------------------------------------
-// v2: zero-guarded copies and lean inner loops.
+// Instances
 // ---------------------------------------------------------------------------
-// Lr[z][i][kPadL + k] = img[z][i][k], Lc[z][i][kPadL + k] = img[z][k][i];
-// guard words are zero.  Stride wl = n + 2*kPadL.
-__global__ void dd_pad_image_kernel(const float *__restrict__ img, float *__restrict__ Lr,
-                                    float *__restrict__ Lc, int n, int wl) {
-  __shared__ float tile[32][33];
-  const size_t z = blockIdx.z;
-  const float *src = img + z * (size_t)n * n;
-  float *dr = Lr + z * (size_t)n * wl, *dc = Lc + z * (size_t)n * wl;
-  const int x = blockIdx.x * 32 + threadIdx.x, y0 = blockIdx.y * 32;
-  for (int dy = threadIdx.y; dy < 32; dy += blockDim.y) {
-    const int y = y0 + dy;
-    float v = 0.0f;
-    if (x < n && y < n) v = src[(size_t)y * n + x];
-    tile[dy][threadIdx.x] = v;
-    if (y < n && x < n) dr[(size_t)y * wl + kPadL + x] = v;
-  }
-  __syncthreads();
-  const int ox = blockIdx.y * 32 + threadIdx.x;
-  for (int dy = threadIdx.y; dy < 32; dy += blockDim.y) {
-    const int oy = blockIdx.x * 32 + dy;
-    if (ox < n && oy < n) dc[(size_t)oy * wl + kPadL + ox] = tile[threadIdx.x][dy];
-  }
-  // guards: the blocks of the first column of tiles zero both ends of their rows
-  if (blockIdx.x == 0) {
-    for (int dy = threadIdx.y; dy < 32; dy += blockDim.y) {
-      const int y = y0 + dy;
-      if (y < n && threadIdx.x < 2 * kPadL) {
-        const int col = threadIdx.x < kPadL ? threadIdx.x : n + threadIdx.x;
-        dr[(size_t)y * wl + col] = 0.0f;
-        dc[(size_t)y * wl + col] = 0.0f;
-      }
-    }
-  }
-}
-
-// Sp[z][v][pads + m] = sino[z][na-1-v... the row of angle v][m]; guards zero.
-__global__ void dd_pad_sino_kernel(const float *__restrict__ sino, float *__restrict__ Sp,
-                                   const DdAngle *__restrict__ tab, int n, int na, int w, int pads) {
-  const int v = blockIdx.y;
-  const size_t z = blockIdx.z;
-  const float *src = sino + z * (size_t)na * n + (size_t)tab[v].out_row * n;
-  float *dst = Sp + z * (size_t)na * w + (size_t)v * w;
-  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < w; c += gridDim.x * blockDim.x) {
-    const int m = c - pads;
-    dst[c] = (m >= 0 && m < n) ? src[m] : 0.0f;
-  }
-}
-
-// Line prefix sums in double, interleaved with the line values:
-// SL[line][kk] = {S(kk), L[kk]} for kk in [-1, n], S(kk) = sum_{j < kk} L[j],
-// with the guards SL[-1] = {0, 0} and SL[n] = {S(n), 0}.  The integral of a
-// line from its start to a boundary D inside pixel kk is then
-// F(D) = S(kk) + (D - P_kk) L[kk] for every kk in [-1, n] (pixel widths 1).
-// One block per line; passes of 256 values, each a fixed-order block scan,
-// so the sums are deterministic.
+constexpr int kGrpDet = 127;              // detectors per forward item (128 boundaries, 4 per lane)
+constexpr int kTileW = 16, kTileH = 8;    // pixels per adjoint item (2x2 per lane, 8x4 lanes)
 constexpr int kScanThreads = 256;
-__global__ void __launch_bounds__(kScanThreads) dd_prefix_kernel(const float *__restrict__ L,
-                                                                 double2 *__restrict__ SL, int n, int wl,
-                                                                 int wsl) {
-  __shared__ double wsum[kScanThreads / 32];
-  __shared__ double carry_s;
-  const size_t line = blockIdx.x;
-  const float *src = L + line * wl + kPadL;
-  double2 *dst = SL + line * wsl + 1;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  double carry = 0.0;
-  for (int base = 0; base < n; base += kScanThreads) {
-    const int k = base + tid;
-    const float vf = k < n ? src[k] : 0.0f;
-    double x = (double)vf;  // inclusive warp scan
-    for (int o = 1; o < 32; o <<= 1) {
-      const double y = __shfl_up_sync(0xffffffffu, x, o);
-      if (lane >= o) x += y;
-    }
-    if (lane == 31) wsum[warp] = x;
-    __syncthreads();
-    double before = carry;  // carry + totals of the earlier warps, in warp order
-    for (int w = 0; w < warp; ++w) before += wsum[w];
-    if (k < n) dst[k] = make_double2(before + (x - (double)vf), (double)vf);
-    if (tid == kScanThreads - 1) carry_s = before + x;
-    __syncthreads();
-    carry = carry_s;
+constexpr int kColWarps = 4, kColRows = 16;
+// Adding 1.5 * 2^23 rounds a float of magnitude < 2^22 to an integer held in
+// the low mantissa bits: int = bits - kMagicBits.
+constexpr float kMagic = 12582912.0f;
+constexpr int kMagicBits = 0x4B400000;
+
+struct DdInst {
+  long long img, sino;   // offsets (floats) of the image / sinogram in the packed arrays
+  long long sl;          // offset (double2) of the row prefix lines; column lines follow
+  long long as;          // offset (double2) of the sinogram prefix rows [na][w2]
+  long long f0, a0;      // first forward / adjoint work item
+  long long r0, c0, s0;  // first row-prefix / column-prefix / sinogram-prefix block
+  const DdAngle *ang;    // [na] per-angle geometry, angle order
+  const float4 *tab;     // adjoint lines: ROWS angles then COLS angles {r, k, z, v*w2 (int bits)}
+  const int2 *tabS;      // adjoint sums: {mode, v*w2}
+  int n, nh, na, pads, w2, nR, nC, nS, ngrp, tx, ty, unused;
+};
+
+// Index of the instance whose range [key, next key) holds item (keys ascend).
+__device__ __forceinline__ int find_inst(const DdInst *__restrict__ inst, int ninst, long long item,
+                                         long long DdInst::*key) {
+  int lo = 0, hi = ninst - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (inst[mid].*key <= item) lo = mid;
+    else hi = mid - 1;
   }
-  if (tid == 0) {
-    dst[-1] = make_double2(0.0, 0.0);
-    dst[n] = make_double2(carry, 0.0);
+  return lo;
+}
+
+// The piece of a line that the reference never credits: the last gap of its
+// boundary walk, ending at min(P_n, D_n) (radon_dd.c:176-177).  If P_n <= D_n
+// it is the overlap of pixel n-1 with the detector m holding P_n
+// (D_m < P_n <= D_m+1); otherwise the overlap of detector n-1 with the pixel k
+// holding D_n (P_k < D_n < P_k+1; if D_n falls on a pixel boundary no piece
+// is lost).  Returns false when nothing is lost, including lines that do not
+// meet the detector range.
+struct DdDrop {
+  int pix, det;
+  float gap;
+};
+__device__ __noinline__ bool dd_dropped_piece(float q, float r, int n, int nh, DdDrop &d) {
+  const float Pn = pix_bound(n, nh, q), Dn = det_bound(n, nh, r);
+  if (Pn <= Dn) {
+    int m = min(max(__float2int_rd(__fdiv_rn(Pn, r)) + nh, -1), n - 1);
+    for (int it = 0; it < 8 && m >= 0 && !(det_bound(m, nh, r) < Pn); ++it) --m;
+    for (int it = 0; it < 8 && m < n - 1 && !(Pn <= det_bound(m + 1, nh, r)); ++it) ++m;
+    if (m < 0) return false;
+    d.pix = n - 1;
+    d.det = m;
+    d.gap = __fsub_rn(Pn, fmaxf(pix_bound(n - 1, nh, q), det_bound(m, nh, r)));
+    return true;
   }
+  int k = min(max(__float2int_rd(__fadd_rn(__fadd_rn(Dn, q), (float)nh)), -1), n - 1);
+  for (int it = 0; it < 8 && k >= 0 && !(pix_bound(k, nh, q) < Dn); ++it) --k;
+  for (int it = 0; it < 8 && k < n - 1 && !(Dn <= pix_bound(k + 1, nh, q)); ++it) ++k;
+  if (k < 0 || Dn == pix_bound(k + 1, nh, q)) return false;
+  d.pix = k;
+  d.det = n - 1;
+  d.gap = __fsub_rn(Dn, fmaxf(det_bound(n - 1, nh, r), pix_bound(k, nh, q)));
+  return true;
 }
 
 // Lines i of [0, n) with q_i = ((i - nh) + 0.5) k inside [qlo, qhi], widened
@@ -301,191 +229,382 @@ __device__ __forceinline__ void dd_line_range(double qlo, double qhi, double k, 
   ib = fhi > (double)(n - 1) ? n - 1 : (fhi < 0.0 ? -1 : (int)fhi);
 }
 
-// Forward.  A warp owns 31 consecutive detectors (lane 31 only supplies the
-// upper boundary of lane 30).  Lane j accumulates T_j = sum over lines of
-// F(D_j) at its lower boundary, and detector m = T_m+1 - T_m: one integral
-// evaluation per line and detector, whatever the detector's width.  The lines
-// on which the dropped last piece of the line can belong to one of the warp's
-// detectors (P_n within the warp's detector span, or beyond D_n for the warp
-// holding detector n-1) form one contiguous band; there every lane walks the
-// pieces exactly instead.
-constexpr int kFwdDet = 31;
-constexpr int kFwdWarps = 4;
-__global__ void __launch_bounds__(32 * kFwdWarps) dd_forward_v4_kernel(
-    const float *__restrict__ Lr, const float *__restrict__ Lc, const double2 *__restrict__ SLr,
-    const double2 *__restrict__ SLc, float *__restrict__ sino, const DdAngle *__restrict__ tab, int n,
-    int nh, int na, int wl, int wsl, FwdEpi ep) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int mA = (blockIdx.x * kFwdWarps + warp) * kFwdDet;
-  const int m = mA + lane;
-  const int v = blockIdx.y;
-  const size_t z = blockIdx.z;
-  const bool live = lane < kFwdDet && m < n;
-  const DdAngle g = tab[v];
-  float acc = 0.0f;
-  const float *Rz = Lr + z * (size_t)n * wl + kPadL, *Cz = Lc + z * (size_t)n * wl + kPadL;
-  if (g.mode == DD_ROWSUM) {
-    if (live)
-      for (int j = 0; j < n; ++j) acc += __ldg(Cz + (size_t)j * wl + m);
-  } else if (g.mode == DD_COLSUM) {
-    if (live)
-      for (int j = 0; j < n; ++j) acc += __ldg(Rz + (size_t)j * wl + m);
-  } else if ((g.mode == DD_ROWS || g.mode == DD_COLS) && mA < n) {
-    const float *L = g.mode == DD_ROWS ? Rz : Cz;
-    const double2 *SL = (g.mode == DD_ROWS ? SLr : SLc) + z * (size_t)n * wsl + 1;
+// ---------------------------------------------------------------------------
+// Pre-passes: prefix sums of the image lines and of the sinogram rows
+// ---------------------------------------------------------------------------
+// Inclusive scan of x over the block (kScanThreads threads), added to carry;
+// returns carry + sum of the values before this thread's and updates carry to
+// carry + block total.  Fixed order, so the result is deterministic.
+__device__ __forceinline__ double block_exclusive_scan(double x, double &carry, double *wsum,
+                                                       double *carry_s) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const double x0 = x;
+  for (int o = 1; o < 32; o <<= 1) {
+    const double y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) wsum[warp] = x;
+  __syncthreads();
+  double before = carry;
+  for (int w = 0; w < warp; ++w) before += wsum[w];
+  if (tid == kScanThreads - 1) *carry_s = before + x;
+  __syncthreads();
+  carry = *carry_s;
+  return before + (x - x0);
+}
+
+// Row lines: work[sl + line*(n+2) + 1 + kk] = {S(kk), L[kk]}, kk in [-1, n],
+// S(kk) = sum_{j<kk} L[j], L the image row; guards {0, 0} and {S(n), 0}.
+__global__ void __launch_bounds__(kScanThreads) dd_row_prefix_kernel(const DdInst *__restrict__ inst,
+                                                                     int ninst, const float *__restrict__ img,
+                                                                     double2 *__restrict__ work) {
+  __shared__ double wsum[kScanThreads / 32];
+  __shared__ double carry_s;
+  const long long b = blockIdx.x;
+  const DdInst &I = inst[find_inst(inst, ninst, b, &DdInst::r0)];
+  const int n = I.n, line = (int)(b - I.r0);
+  const float *src = img + I.img + (size_t)line * n;
+  double2 *dst = work + I.sl + (size_t)line * (n + 2) + 1;
+  double carry = 0.0;
+  for (int base = 0; base < n; base += kScanThreads) {
+    const int k = base + threadIdx.x;
+    const float v = k < n ? __ldg(src + k) : 0.0f;
+    const double ex = block_exclusive_scan((double)v, carry, wsum, &carry_s);
+    if (k < n) dst[k] = make_double2(ex, (double)v);
+  }
+  if (threadIdx.x == 0) {
+    dst[-1] = make_double2(0.0, 0.0);
+    dst[n] = make_double2(carry, 0.0);
+  }
+}
+
+// Column lines (line c = image column c), 32 columns per block: each warp
+// sums a quarter of the rows, then rescans its rows 16 at a time through
+// shared memory so that each column line is written contiguously.
+__global__ void __launch_bounds__(32 * kColWarps) dd_col_prefix_kernel(const DdInst *__restrict__ inst,
+                                                                       int ninst, const float *__restrict__ img,
+                                                                       double2 *__restrict__ work) {
+  __shared__ double tot[kColWarps][32];
+  __shared__ double2 tile[kColWarps][kColRows][33];
+  const long long b = blockIdx.x;
+  const DdInst &I = inst[find_inst(inst, ninst, b, &DdInst::c0)];
+  const int n = I.n, c0 = (int)(b - I.c0) * 32;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int col = c0 + lane;
+  const float *im = img + I.img;
+  double2 *SLc = work + I.sl + (size_t)n * (n + 2) + 1;
+  const int ch = (n + kColWarps - 1) / kColWarps;
+  const int r0 = min(w * ch, n), r1 = min(r0 + ch, n);
+  double t = 0.0;
+  if (col < n)
+    for (int r = r0; r < r1; ++r) t += (double)__ldg(im + (size_t)r * n + col);
+  tot[w][lane] = t;
+  __syncthreads();
+  double run = 0.0, total = 0.0;
+  for (int u = 0; u < kColWarps; ++u) {
+    if (u < w) run += tot[u][lane];
+    total += tot[u][lane];
+  }
+  for (int rb = r0; rb < r1; rb += kColRows) {
+    for (int rr = 0; rr < kColRows; ++rr) {
+      const int r = rb + rr;
+      const float v = (col < n && r < r1) ? __ldg(im + (size_t)r * n + col) : 0.0f;
+      tile[w][rr][lane] = make_double2(run, (double)v);
+      run += (double)v;
+    }
+    __syncwarp();
+    for (int cc2 = 0; cc2 < 16; ++cc2) {
+      const int cc = 2 * cc2 + (lane >> 4), rr = lane & 15;
+      const int cg = c0 + cc, r = rb + rr;
+      if (cg < n && r < r1) SLc[(size_t)cg * (n + 2) + r] = tile[w][rr][cc];
+    }
+    __syncwarp();
+  }
+  if (w == 0 && col < n) {
+    SLc[(size_t)col * (n + 2) - 1] = make_double2(0.0, 0.0);
+    SLc[(size_t)col * (n + 2) + n] = make_double2(total, 0.0);
+  }
+}
+
+// Sinogram rows, one block per angle v: entry e = m + pads (m in
+// [-pads, n + pads)) holds {D_m, S_m, D_m+1, S_m+1}, the detector boundaries
+// and values (S = 0 outside [0, n)) that a pixel starting in detector m
+// overlaps.  Row / column-sum angles only use S_m.
+__global__ void __launch_bounds__(kScanThreads) dd_sino_expand_kernel(const DdInst *__restrict__ inst,
+                                                                      int ninst, const float *__restrict__ sino,
+                                                                      double2 *__restrict__ work) {
+  const long long b = blockIdx.x;
+  const DdInst &I = inst[find_inst(inst, ninst, b, &DdInst::s0)];
+  const int v = (int)(b - I.s0), n = I.n, nh = I.nh, pads = I.pads, w2 = I.w2;
+  const DdAngle g = I.ang[v];
+  const float *src = sino + I.sino + (size_t)g.out_row * n;
+  float4 *dst = (float4 *)(work + I.as) + (size_t)v * w2;
+  const bool lines = g.mode == DD_ROWS || g.mode == DD_COLS;
+  for (int e = threadIdx.x; e < w2; e += blockDim.x) {
+    const int m = e - pads;
+    const float s0 = (m >= 0 && m < n) ? __ldg(src + m) : 0.0f;
+    const float s1 = (m + 1 >= 0 && m + 1 < n) ? __ldg(src + m + 1) : 0.0f;
+    dst[e] = lines ? make_float4(det_bound(m, nh, g.r), s0, det_bound(m + 1, nh, g.r), s1)
+                   : make_float4(0.0f, s0, 0.0f, s1);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Forward: a warp item is 127 detectors of one angle; lane l holds the lower
+// boundaries of detectors B0 + 32 j + l (j = 0..3), and T_j = sum over lines of
+// F(boundary).  Lines whose dropped piece may belong to one of the item's
+// detectors form one contiguous band, where the piece is also subtracted.
+// ---------------------------------------------------------------------------
+template <bool BAND>
+__device__ __forceinline__ void dd_fwd_lines(int ia, int ib, const double2 *__restrict__ SL, int ws, float k,
+                                             float r, int n, int nh, int B0, int lane, const float (&Dlo)[4],
+                                             const float (&lo_nh)[4], double (&T)[4], double (&C)[4]) {
+  float y = (float)(ia - nh) + 0.5f;
+  const double2 *sl = SL + (size_t)ia * ws;
+  const float nlim = (float)n + 0.25f, nhf = (float)nh;
+#pragma unroll 2
+  for (int i = ia; i < ib; ++i) {
+    const float q = __fmul_rn(y, k);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      // kk = floor(D + nh + q) clamped to [-1, n], as a float and an int by
+      // rounding at 1.5 * 2^23 (an index one off at a pixel boundary leaves F
+      // unchanged up to rounding, F being continuous)
+      const float t = fminf(fmaxf(__fadd_rn(lo_nh[j], q), -0.5f), nlim);
+      const float f = __fadd_rn(__fadd_rn(t, -0.5f), kMagic);
+      const int kk = __float_as_int(f) - kMagicBits;
+      const float Pk = __fsub_rn(__fsub_rn(__fsub_rn(f, kMagic), nhf), q);
+      const double2 e = __ldg(sl + kk);
+      T[j] = fma((double)__fsub_rn(Dlo[j], Pk), e.y, T[j] + e.x);
+    }
+    if (BAND) {
+      DdDrop d;
+      if (dd_dropped_piece(q, r, n, nh, d)) {
+        const int rel = d.det - B0;
+        if (rel >= 0 && rel < kGrpDet && (rel & 31) == lane) {
+          const double amt = (double)d.gap * __ldg(&sl[d.pix].y);
+          const int jj = rel >> 5;
+#pragma unroll
+          for (int j = 0; j < 4; ++j)
+            if (j == jj) C[j] += amt;
+        }
+      }
+    }
+    y = __fadd_rn(y, 1.0f);
+    sl += ws;
+  }
+}
+
+__device__ __forceinline__ void dd_fwd_item(const DdInst &I, int v, int grp, int lane,
+                                            const double2 *__restrict__ work, float *__restrict__ sino,
+                                            const FwdEpi &ep, long long slot) {
+  const DdAngle g = I.ang[v];
+  const int n = I.n, nh = I.nh, ws = n + 2;
+  const int B0 = grp * kGrpDet;
+  const double2 *SLr = work + I.sl + 1, *SLc = SLr + (size_t)n * ws;
+  float acc[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+  if (g.mode == DD_ROWSUM || g.mode == DD_COLSUM) {
+    // detector m <- total of image row m (ROWSUM) or column m (COLSUM)
+    const double2 *SL = g.mode == DD_ROWSUM ? SLr : SLc;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int m = B0 + 32 * j + lane;
+      if (32 * j + lane < kGrpDet && m < n) acc[j] = (float)__ldg(&SL[(size_t)m * ws + n].x);
+    }
+  } else if (g.mode == DD_ROWS || g.mode == DD_COLS) {
+    const double2 *SL = g.mode == DD_ROWS ? SLr : SLc;
     const float r = g.r, k = g.k;
-    const float Dlo = det_bound(m, nh, r), Dhi = det_bound(m + 1, nh, r);
-    const float Dn = det_bound(n, nh, r);
-    const int mB = min(mA + kFwdDet - 1, n - 1);
-    const double DA = (double)det_bound(mA, nh, r), DB = (double)det_bound(mB + 1, nh, r);
+    float Dlo[4], lo_nh[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      Dlo[j] = det_bound(B0 + 32 * j + lane, nh, r);
+      lo_nh[j] = __fadd_rn(Dlo[j], (float)nh);
+    }
+    const int mEnd = min(B0 + kGrpDet, n);
+    const double DA = (double)det_bound(B0, nh, r), DB = (double)det_bound(mEnd, nh, r);
     const double kd = (double)k, PN = (double)(n - nh);
     int i0, i1, j0, j1;
     dd_line_range(-(double)nh - DB, PN - DA, kd, n, nh, i0, i1);
     const double margin = 2.0 + 1e-6 * (fabs(DA) + fabs(DB) + (double)n * (1.0 + fabs(kd)));
-    const double BL = DA - margin, BH = mB == n - 1 ? 1e30 : DB + margin;
-    dd_line_range(PN - BH, PN - BL, kd, n, nh, j0, j1);
+    dd_line_range(PN - (mEnd == n ? 1e30 : DB + margin), PN - (DA - margin), kd, n, nh, j0, j1);
     j0 = max(j0, i0);
     j1 = min(j1, i1);
-    if (j0 > j1) {  // no band: all lines are fast
+    if (j0 > j1) {
       j0 = i1 + 1;
       j1 = i1;
     }
-    const float lo_nh = __fadd_rn(Dlo, (float)nh);
-    double T = 0.0, X = 0.0;
-    for (int seg = 0; seg < 2; ++seg) {
-      const int ia = seg == 0 ? i0 : j1 + 1, ib = seg == 0 ? j0 : i1 + 1;
-      float y = (float)(ia - nh) + 0.5f;
-      const double2 *sl = SL + (size_t)ia * wsl;
-#pragma unroll 4
-      for (int i = ia; i < ib; ++i) {
-        const float q = __fmul_rn(y, k);
-        const int kk = min(max(__float2int_rd(__fadd_rn(lo_nh, q)), -1), n);
-        const float Pk = __fsub_rn((float)(kk - nh), q);
-        const double2 e = __ldg(sl + kk);
-        T = fma((double)__fsub_rn(Dlo, Pk), e.y, T + e.x);
-        y = __fadd_rn(y, 1.0f);
-        sl += wsl;
-      }
+    double T[4] = {0.0, 0.0, 0.0, 0.0}, C[4] = {0.0, 0.0, 0.0, 0.0};
+    dd_fwd_lines<false>(i0, j0, SL, ws, k, r, n, nh, B0, lane, Dlo, lo_nh, T, C);
+    dd_fwd_lines<true>(j0, j1 + 1, SL, ws, k, r, n, nh, B0, lane, Dlo, lo_nh, T, C);
+    dd_fwd_lines<false>(j1 + 1, i1 + 1, SL, ws, k, r, n, nh, B0, lane, Dlo, lo_nh, T, C);
+    // the upper boundary of detector B0 + 32 j + l is lane l+1's j-th, or lane 0's (j+1)-th
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const double a = __shfl_down_sync(0xffffffffu, T[j], 1);
+      const double b = __shfl_sync(0xffffffffu, j < 3 ? T[j < 3 ? j + 1 : 3] : 0.0, 0);
+      const double up = lane < 31 ? a : b;
+      acc[j] = (float)((up - T[j]) - C[j]);
     }
-    if (live) {
-      float y = (float)(j0 - nh) + 0.5f;
-      for (int i = j0; i <= j1; ++i, y = __fadd_rn(y, 1.0f))
-        X += (double)dd_fwd_line_exact(L + (size_t)i * wl, m, __fmul_rn(y, k), r, Dlo, Dhi, Dn, n, nh);
-    }
-    const double Tup = __shfl_down_sync(0xffffffffu, T, 1);
-    acc = (float)((Tup - T) + X);
   }
-  fwd_store(ep, acc, live, z * (size_t)na * n + (size_t)g.out_row * n + (live ? m : 0), sino);
+  double r2 = 0.0;
+  const size_t row = (size_t)I.sino + (size_t)g.out_row * n;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const int m = B0 + 32 * j + lane;
+    if (32 * j + lane < kGrpDet && m < n) sino[row + m] = fwd_apply(ep, acc[j], row + m, r2);
+  }
+  fwd_resid_commit(ep, r2, (size_t)slot);
 }
 
-constexpr int kAdjChunk = 1024;
-
-// One line segment of two pixels [P0, P1], [P1, P2] (the line's offset q is
-// applied); adds their weights times the detector values into a0, a1.  Exact
-// unless the segment touches the last pixel or detector, where the caller
-// takes dd_adj_pixel_exact instead.
-__device__ __forceinline__ void dd_adj_segment(float P0, float P1, float P2, const float4 e,
-                                               const float *__restrict__ S, float nhp, int pads, int n,
-                                               float &a0, float &a1, bool &edge) {
-  const float r = e.x;
-  int mp = (int)floorf(fmaf(P0, e.z, nhp));
-  float fm = __fsub_rn((float)mp, nhp);
-  float Dm = __fmul_rn(fm, r);
-  if (Dm > P0) {
-    --mp;
-    fm = __fsub_rn(fm, 1.0f);
-    Dm = __fmul_rn(fm, r);
+// Work fetch.  BLOCK: a block takes W consecutive items at a time (for the
+// forward, consecutive angles of one detector group, whose warps read nearly
+// the same prefix lines, which then hit in L1); otherwise each warp takes one
+// item.  The autotuner picks the mode; results do not depend on it.
+template <bool BLOCK>
+__device__ __forceinline__ long long fetch_item(unsigned long long *ctr, int W, long long *slot) {
+  if (BLOCK) {
+    if (threadIdx.x == 0) *slot = (long long)atomicAdd(ctr, (unsigned long long)W);
+    __syncthreads();
+    const long long b = *slot;
+    __syncthreads();
+    return b + (threadIdx.x >> 5);
   }
-  float D1 = __fmul_rn(__fadd_rn(fm, 1.0f), r);
-  if (D1 <= P0) {
-    ++mp;
-    fm = __fadd_rn(fm, 1.0f);
-    D1 = __fmul_rn(__fadd_rn(fm, 1.0f), r);
-  }
-  edge = (unsigned)(mp - pads - (n - 3)) <= 2u;  // the segment meets detector n-1
-  const float D2 = __fmul_rn(__fadd_rn(fm, 2.0f), r);
-  const float *sp = S + __float_as_int(e.w) + mp;
-  const float v0 = __ldg(sp), v1 = __ldg(sp + 1), v2 = __ldg(sp + 2);
-  const float t0 = fminf(D1, P1);
-  a0 = fmaf(__fsub_rn(t0, P0), v0, a0);
-  a0 = fmaf(__fsub_rn(P1, t0), v1, a0);
-  const bool c = P1 >= D1;
-  const float Da = c ? D2 : D1, va = c ? v1 : v0, vb = c ? v2 : v1;
-  const float t1 = fminf(Da, P2);
-  a1 = fmaf(__fsub_rn(t1, P1), va, a1);
-  a1 = fmaf(__fsub_rn(P2, t1), vb, a1);
+  unsigned long long it = 0;
+  if ((threadIdx.x & 31) == 0) it = atomicAdd(ctr, 1ull);
+  return (long long)__shfl_sync(0xffffffffu, it, 0);
 }
 
-// Adjoint: one thread per 2x2 pixel tile (rows a0, a0+1; columns b0, b0+1).
-// For a ROWS angle the tile is two row segments of two pixels, for a COLS
-// angle two column segments; each segment shares its boundary and detector
-// arithmetic between its two pixels.
-__global__ void __launch_bounds__(256) dd_adjoint_v3_kernel(
-    const float *__restrict__ Sp, float *__restrict__ img, const float4 *__restrict__ tabR, int nR,
-    const float4 *__restrict__ tabC, int nC, const int2 *__restrict__ tabS, int nS, int n, int nh,
-    int na, int w, int pads, AdjEpi ep) {
-  __shared__ float4 st[kAdjChunk];
-  const int b0 = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
-  const int a0 = 2 * (blockIdx.y * blockDim.y + threadIdx.y);
-  const size_t z = blockIdx.z;
-  const bool any = a0 < n && b0 < n;
-  const float *S = Sp + z * (size_t)na * w;
-  const int tid = threadIdx.y * blockDim.x + threadIdx.x, nthr = blockDim.x * blockDim.y;
-  const float nhp = (float)(nh + pads);
-  float acc[2][2] = {{0.f, 0.f}, {0.f, 0.f}};  // [row - a0][col - b0]
-  for (int pass = 0; pass < 2; ++pass) {
-    const float4 *tab = pass == 0 ? tabR : tabC;
-    const int cnt_all = pass == 0 ? nR : nC;
-    // ROWS: lines are rows a0, a0+1 and the segment is columns b0, b0+1; COLS: transposed
-    const int l0 = pass == 0 ? a0 : b0, k0 = pass == 0 ? b0 : a0;
-    const float y0 = (float)(l0 - nh) + 0.5f, y1 = __fadd_rn(y0, 1.0f);
-    const float x0 = (float)(k0 - nh), x1 = __fadd_rn(x0, 1.0f), x2 = __fadd_rn(x0, 2.0f);
-    const bool edge_pixel = k0 + 1 >= n - 1;
-    for (int v0 = 0; v0 < cnt_all; v0 += kAdjChunk) {
-      const int cnt = min(kAdjChunk, cnt_all - v0);
-      __syncthreads();
-      for (int t = tid; t < cnt; t += nthr) st[t] = tab[v0 + t];
-      __syncthreads();
-      if (!any) continue;
-      for (int u = 0; u < cnt; ++u) {
-        const float4 e = st[u];
-        for (int li = 0; li < 2; ++li) {
-          if (l0 + li >= n) break;  // odd n: the tile's second line is outside the image
-          const float q = __fmul_rn(li ? y1 : y0, e.y);
-          const float P0 = __fsub_rn(x0, q), P1 = __fsub_rn(x1, q), P2 = __fsub_rn(x2, q);
-          float s0 = 0.0f, s1 = 0.0f;
-          bool edge;
-          dd_adj_segment(P0, P1, P2, e, S, nhp, pads, n, s0, s1, edge);
-          if (edge || edge_pixel) {
-            const float *srow = S + __float_as_int(e.w) + pads;
-            s0 = dd_adj_pixel_exact(srow, k0, q, e.x, n, nh);
-            s1 = k0 + 1 < n ? dd_adj_pixel_exact(srow, k0 + 1, q, e.x, n, nh) : 0.0f;
-          }
-          if (pass == 0) {
-            acc[li][0] += s0;
-            acc[li][1] += s1;
-          } else {
-            acc[0][li] += s0;
-            acc[1][li] += s1;
-          }
+// Detector groups are taken centre first: central groups meet the most lines,
+// so the long items run first and the short ones fill the tail.
+__device__ __forceinline__ int centre_out(int gi, int ngrp) {
+  const int c = (ngrp - 1) >> 1;
+  return (gi & 1) ? c + ((gi + 1) >> 1) : c - (gi >> 1);
+}
+
+template <int W, bool BLOCK>
+__global__ void __launch_bounds__(32 * W) dd_fwd_kernel(const DdInst *__restrict__ inst, int ninst,
+                                                         long long nitems, unsigned long long *__restrict__ ctr,
+                                                         const double2 *__restrict__ work,
+                                                         float *__restrict__ sino, FwdEpi ep) {
+  __shared__ long long base_s;
+  const int lane = threadIdx.x & 31;
+  for (;;) {
+    const long long item = fetch_item<BLOCK>(ctr, W, &base_s);
+    if (item - (BLOCK ? (threadIdx.x >> 5) : 0) >= nitems) break;  // block-uniform under BLOCK
+    if (item < nitems) {
+      const DdInst &I = inst[find_inst(inst, ninst, item, &DdInst::f0)];
+      const int local = (int)(item - I.f0);
+      dd_fwd_item(I, local % I.na, centre_out(local / I.na, I.ngrp), lane, work, sino, ep, item);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Adjoint: a warp item is a 16x8 pixel tile; lane l holds the 2x2 pixels at
+// rows a0, a0+1 and columns b0, b0+1.  Per angle and line each pixel [P0, P1]
+// overlaps the detector a holding P0 and possibly a+1 (detectors are at least
+// one pixel wide): (min(D_a+1, P1) - P0) S_a + (P1 - min(D_a+1, P1)) S_a+1,
+// the reference's two gaps.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float dd_adj_pixel(float P0, float P1, float z, float cm,
+                                              const float4 *__restrict__ rowm) {
+  // a = floor(P0 z + nh) by rounding at 1.5 * 2^23, read as the float's bits
+  // (rowm is the row base minus kMagicBits entries); one off at a detector
+  // boundary only moves a zero-width piece
+  const float4 t = __ldg(rowm + __float_as_int(__fadd_rn(__fmaf_rn(P0, z, -0.5f), cm)));
+  // t = {D_a, S_a, D_a+1, S_a+1}
+  const float m = fminf(t.z, P1);
+  return fmaf(__fsub_rn(P1, m), t.w, __fmul_rn(__fsub_rn(m, P0), t.y));
+}
+
+template <bool COLS>
+__device__ __forceinline__ void dd_adj_pass(const float4 *__restrict__ tab, int cnt,
+                                            const float4 *__restrict__ AS, int a0, int b0, int n, int nh,
+                                            float (&acc)[2][2]) {
+  const int l0 = COLS ? b0 : a0, k0 = COLS ? a0 : b0;
+  const float y0 = (float)(l0 - nh) + 0.5f, y1 = __fadd_rn(y0, 1.0f);
+  const float x0 = (float)(k0 - nh), x1 = __fadd_rn(x0, 1.0f), x2 = __fadd_rn(x0, 2.0f);
+  const bool lastpix = k0 + 1 >= n - 1;
+  const float cm = kMagic + (float)nh;
+#pragma unroll 2
+  for (int u = 0; u < cnt; ++u) {
+    const float4 e = __ldg(tab + u);
+    const float r = e.x, k = e.y, z = e.z;
+    const float4 *row = AS + __float_as_int(e.w);
+    const float4 *rowm = row - kMagicBits;
+    const float Dn = det_bound(n, nh, r);
+#pragma unroll
+    for (int li = 0; li < 2; ++li) {
+      const float q = __fmul_rn(li ? y1 : y0, k);
+      const float P0 = __fsub_rn(x0, q), P1 = __fsub_rn(x1, q), P2 = __fsub_rn(x2, q);
+      float s0 = dd_adj_pixel(P0, P1, z, cm, rowm), s1 = dd_adj_pixel(P1, P2, z, cm, rowm);
+      if (lastpix || (P0 < Dn && Dn < P2)) {
+        DdDrop d;
+        if (dd_dropped_piece(q, r, n, nh, d)) {
+          const float sd = __fmul_rn(d.gap, __ldg(&row[d.det].y));
+          if (d.pix == k0) s0 -= sd;
+          else if (d.pix == k0 + 1) s1 -= sd;
         }
       }
+      if (COLS) {
+        acc[0][li] += s0;
+        acc[1][li] += s1;
+      } else {
+        acc[li][0] += s0;
+        acc[li][1] += s1;
+      }
     }
   }
-  if (any) {
-    for (int t = 0; t < nS; ++t) {  // row / column sums (|sin| or |cos| < 1e-7)
-      const int2 e = __ldg(tabS + t);
-      const float *srow = S + e.y + pads;
-      for (int dr = 0; dr < 2; ++dr)
-        for (int dc = 0; dc < 2; ++dc) acc[dr][dc] += __ldg(srow + (e.x == DD_ROWSUM ? a0 + dr : b0 + dc));
-    }
+}
+
+__device__ __forceinline__ void dd_adj_item(const DdInst &I, int txi, int tyi, int lane,
+                                            const double2 *__restrict__ work, float *__restrict__ img,
+                                            const AdjEpi &ep) {
+  const int n = I.n, nh = I.nh;
+  const int b0 = txi * kTileW + 2 * (lane & 7), a0 = tyi * kTileH + 2 * (lane >> 3);
+  float acc[2][2] = {{0.0f, 0.0f}, {0.0f, 0.0f}};
+  const float4 *AS = (const float4 *)(work + I.as) + I.pads;
+  // tiles that start outside the image (n not a multiple of the tile) only
+  // take part in the epilogue's warp reductions
+  const bool inside = a0 < n && b0 < n;
+  if (inside) {
+    dd_adj_pass<false>(I.tab, I.nR, AS, a0, b0, n, nh, acc);
+    dd_adj_pass<true>(I.tab + I.nR, I.nC, AS, a0, b0, n, nh, acc);
   }
-  for (int dr = 0; dr < 2; ++dr)
-    for (int dc = 0; dc < 2; ++dc) {
-      const int a = a0 + dr, b = b0 + dc;
+  for (int t = 0; inside && t < I.nS; ++t) {  // row / column sums (|sin| or |cos| < 1e-7)
+    const int2 e = __ldg(I.tabS + t);
+    const float4 *row = AS + e.y;
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+      for (int j = 0; j < 2; ++j) acc[i][j] += __ldg(&row[e.x == DD_ROWSUM ? a0 + i : b0 + j].y);
+  }
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      const int a = a0 + i, b = b0 + j;
       const bool live = a < n && b < n;
-      adj_store(ep, acc[dr][dc], live, z * (size_t)n * n + (size_t)(live ? a : 0) * n + (live ? b : 0), img);
+      adj_store(ep, acc[i][j], live, (size_t)I.img + (size_t)(live ? a : 0) * n + (live ? b : 0), img);
     }
+}
+
+template <int W, bool BLOCK>
+__global__ void __launch_bounds__(32 * W) dd_adj_kernel(const DdInst *__restrict__ inst, int ninst,
+                                                         long long nitems, unsigned long long *__restrict__ ctr,
+                                                         const double2 *__restrict__ work,
+                                                         float *__restrict__ img, AdjEpi ep) {
+  __shared__ long long base_s;
+  const int lane = threadIdx.x & 31;
+  for (;;) {
+    const long long item = fetch_item<BLOCK>(ctr, W, &base_s);
+    if (item - (BLOCK ? (threadIdx.x >> 5) : 0) >= nitems) break;
+    if (item < nitems) {
+      const DdInst &I = inst[find_inst(inst, ninst, item, &DdInst::a0)];
+      const int local = (int)(item - I.a0);
+      dd_adj_item(I, local % I.tx, local / I.tx, lane, work, img, ep);
+    }
+  }
 }
 
 }  // namespace
@@ -535,94 +654,350 @@ int dd_forward_launch(const float *d_img, float *d_scratch, float *d_sino, const
   return TOMO_OK;
 }
 
-// Plan layout: d_angles = DdAngle[na] (angle order); d_aux = adjoint tables
-// (float4 ROWS[nR], float4 COLS[nC], int2 SUMS[nS]); d_scratch = Lr | Lc | Sp.
-int dd_setup(Plan &p) {
-  const int na = p.g.na, n = p.g.n, nh = p.nh, nz = p.g.nz;
-  std::vector<DdAngle> tab(na);
-  int rc = dd_build_table(p.angles.data(), na, tab.data());
-  if (rc) return rc;
-  p.dd_pads = (int)std::ceil((nh + 1) * (std::sqrt(2.0) - 1.0)) + 4;
-  p.dd_w = ((n + 2 * p.dd_pads) + 3) / 4 * 4;
-  p.dd_wl = n + 2 * kPadL;
-  std::vector<float4> rows, cols;
-  std::vector<int2> sums;
-  for (int v = 0; v < na; ++v) {
-    const DdAngle &a = tab[v];
-    const int off = v * p.dd_w;
-    if (a.mode == DD_ROWS || a.mode == DD_COLS) {
-      // z = 1/r (= sin or cos): the detector index of a boundary P is about P/r + nh
-      float s, c;
-      sincosf(p.angles[v], &s, &c);
-      float4 e = make_float4(a.r, a.k, a.mode == DD_ROWS ? s : c, 0.0f);
-      std::memcpy(&e.w, &off, sizeof(int));
-      (a.mode == DD_ROWS ? rows : cols).push_back(e);
-    } else if (a.mode == DD_ROWSUM || a.mode == DD_COLSUM) {
-      sums.push_back(make_int2(a.mode, off));
-    }
-  }
-  p.dd_nR = (int)rows.size();
-  p.dd_nC = (int)cols.size();
-  p.dd_nS = (int)sums.size();
-  TOMO_CUDA(cudaMalloc(&p.d_angles, sizeof(DdAngle) * (size_t)na));
-  TOMO_CUDA(cudaMemcpy(p.d_angles, tab.data(), sizeof(DdAngle) * (size_t)na, cudaMemcpyHostToDevice));
-  const size_t aux_bytes = sizeof(float4) * (rows.size() + cols.size()) + sizeof(int2) * (sums.size() + 1);
-  TOMO_CUDA(cudaMalloc(&p.d_aux, aux_bytes));
-  char *aux = (char *)p.d_aux;
-  if (!rows.empty())
-    TOMO_CUDA(cudaMemcpy(aux, rows.data(), sizeof(float4) * rows.size(), cudaMemcpyHostToDevice));
-  if (!cols.empty())
-    TOMO_CUDA(cudaMemcpy(aux + sizeof(float4) * rows.size(), cols.data(), sizeof(float4) * cols.size(),
-                         cudaMemcpyHostToDevice));
-  if (!sums.empty())
-    TOMO_CUDA(cudaMemcpy(aux + sizeof(float4) * (rows.size() + cols.size()), sums.data(),
-                         sizeof(int2) * sums.size(), cudaMemcpyHostToDevice));
-  const size_t lines = 2 * (size_t)nz * n * p.dd_wl, sp = (size_t)nz * na * p.dd_w;
-  const size_t nsum = 2 * (size_t)nz * n * (n + 2);  // double2
-  p.scratch_bytes = (sizeof(float) * (lines + sp) + 255) / 256 * 256 + sizeof(double2) * nsum;
-  // residual partials: one per warp of the forward grid (dd_forward)
-  const int per_block = kFwdDet * kFwdWarps;
-  p.fwd_warps = (size_t)((n + per_block - 1) / per_block) * kFwdWarps * na * nz;
-  TOMO_CUDA(cudaMalloc(&p.d_scratch, p.scratch_bytes));
+namespace {
+
+// Per-plan state: the instance table, the geometry tables of every distinct
+// geometry, the persistent kernels' work counters and the tuned launch shape.
+struct DdState {
+  std::vector<DdInst> inst;  // scheduling order (largest work first)
+  DdInst *d_inst = nullptr;
+  void *d_tables = nullptr;
+  unsigned long long *d_ctr = nullptr;  // [0] forward items, [1] adjoint items
+  long long fwd_items = 0, adj_items = 0, row_blocks = 0, col_blocks = 0, sino_blocks = 0;
+  double updates = 0.0;  // pixel x angle updates per application
+  int wf = 1, wa = 1;    // launch shape (kDdCfg index) of the forward / adjoint kernels
+  int grid_f = 0, grid_a = 0;
+  std::vector<size_t> img_off, sino_off;  // packed offsets in the caller's order (count + 1)
+  std::string tuning;
+};
+
+void dd_state_free(void *q) {
+  auto *S = (DdState *)q;
+  if (S->d_inst) cudaFree(S->d_inst);
+  if (S->d_tables) cudaFree(S->d_tables);
+  if (S->d_ctr) cudaFree(S->d_ctr);
+  delete S;
+}
+
+using FwdFn = void (*)(const DdInst *, int, long long, unsigned long long *, const double2 *, float *,
+                      FwdEpi);
+using AdjFn = void (*)(const DdInst *, int, long long, unsigned long long *, const double2 *, float *,
+                      AdjEpi);
+struct DdCfg {
+  int W;
+  bool block;
+  FwdFn fwd;
+  AdjFn adj;
+};
+// Launch shapes the autotuner chooses from: warps per block x fetch mode.
+const DdCfg kDdCfg[] = {
+    {2, false, dd_fwd_kernel<2, false>, dd_adj_kernel<2, false>},
+    {4, false, dd_fwd_kernel<4, false>, dd_adj_kernel<4, false>},
+    {8, false, dd_fwd_kernel<8, false>, dd_adj_kernel<8, false>},
+    {2, true, dd_fwd_kernel<2, true>, dd_adj_kernel<2, true>},
+    {4, true, dd_fwd_kernel<4, true>, dd_adj_kernel<4, true>},
+    {8, true, dd_fwd_kernel<8, true>, dd_adj_kernel<8, true>},
+};
+constexpr int kNumCfg = (int)(sizeof(kDdCfg) / sizeof(kDdCfg[0]));
+
+std::string cfg_name(int c) { return "w" + std::to_string(kDdCfg[c].W) + (kDdCfg[c].block ? "b" : "w"); }
+
+// Persistent grid: as many blocks as fit on the device at once.
+int dd_grid(int c, bool fwd, int *grid) {
+  int dev = 0, sms = 0, nb = 0;
+  TOMO_CUDA(cudaGetDevice(&dev));
+  TOMO_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  const void *k = fwd ? (const void *)kDdCfg[c].fwd : (const void *)kDdCfg[c].adj;
+  TOMO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, 32 * kDdCfg[c].W, 0));
+  *grid = std::max(1, nb) * sms;
   return TOMO_OK;
 }
 
-// scratch layout: Lr | Lc (floats, nz*n*wl each) | Sp (floats) | SLr | SLc (double2, nz*n*(n+2) each)
-static double2 *dd_sums(Plan &p) {
-  const size_t fl = 2 * (size_t)p.g.nz * p.g.n * p.dd_wl + (size_t)p.g.nz * p.g.na * p.dd_w;
-  const size_t off = (fl * sizeof(float) + 255) / 256 * 256;
-  return (double2 *)((char *)p.d_scratch + off);
-}
-
-int dd_forward(Plan &p, const float *d_img, float *d_sino, cudaStream_t s, const FwdEpi &ep) {
-  const int n = p.g.n, na = p.g.na, nz = p.g.nz, wsl = n + 2;
-  float *Lr = p.d_scratch, *Lc = p.d_scratch + (size_t)nz * n * p.dd_wl;
-  double2 *SLr = dd_sums(p), *SLc = SLr + (size_t)nz * n * wsl;
-  dim3 tb(32, 8), tg((n + 31) / 32, (n + 31) / 32, nz);
-  dd_pad_image_kernel<<<tg, tb, 0, s>>>(d_img, Lr, Lc, n, p.dd_wl);
-  dd_prefix_kernel<<<nz * n, kScanThreads, 0, s>>>(Lr, SLr, n, p.dd_wl, wsl);
-  dd_prefix_kernel<<<nz * n, kScanThreads, 0, s>>>(Lc, SLc, n, p.dd_wl, wsl);
-  const int per_block = kFwdDet * kFwdWarps;
-  dim3 fb(32 * kFwdWarps), fg((n + per_block - 1) / per_block, na, nz);
-  dd_forward_v4_kernel<<<fg, fb, 0, s>>>(Lr, Lc, SLr, SLc, d_sino, (const DdAngle *)p.d_angles, n, p.nh, na,
-                                         p.dd_wl, wsl, ep);
+int dd_launch_fwd(const DdState &S, int c, int grid, const double2 *work, float *sino, cudaStream_t s,
+                  const FwdEpi &ep) {
+  TOMO_CUDA(cudaMemsetAsync(S.d_ctr, 0, sizeof(unsigned long long), s));
+  kDdCfg[c].fwd<<<grid, 32 * kDdCfg[c].W, 0, s>>>(S.d_inst, (int)S.inst.size(), S.fwd_items, S.d_ctr, work,
+                                                    sino, ep);
   TOMO_CUDA(cudaGetLastError());
   return TOMO_OK;
+}
+
+int dd_launch_adj(const DdState &S, int c, int grid, const double2 *work, float *img, cudaStream_t s,
+                  const AdjEpi &ep) {
+  TOMO_CUDA(cudaMemsetAsync(S.d_ctr + 1, 0, sizeof(unsigned long long), s));
+  kDdCfg[c].adj<<<grid, 32 * kDdCfg[c].W, 0, s>>>(S.d_inst, (int)S.inst.size(), S.adj_items, S.d_ctr + 1,
+                                                    work, img, ep);
+  TOMO_CUDA(cudaGetLastError());
+  return TOMO_OK;
+}
+
+// Tuned shapes, shared by plans of the same workload within the process.
+std::mutex g_tune_mu;
+std::map<std::tuple<long long, long long, int, int, int>, std::pair<int, int>> g_tuned;
+
+constexpr double kTuneMinUpdates = 5e7;  // below this the default shape is used untimed
+
+// Chooses the launch shape (warps per block and fetch mode, kDdCfg) of the
+// forward and adjoint kernels by timing each candidate on the plan's own
+// scratch: the scratch is zeroed, the forward reads its prefix-line area and
+// writes into its sinogram-row area, the adjoint the reverse, so no caller
+// buffer is touched.  The choice does not change any result (each output is
+// owned by one lane whatever the shape), only the time.
+int dd_autotune(Plan &p, DdState &S) {
+  const auto key = std::make_tuple(S.fwd_items, S.adj_items, (int)S.inst.size(), S.inst[0].n, S.inst[0].na);
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tuned.find(key);
+    if (it != g_tuned.end()) {
+      S.wf = it->second.first;
+      S.wa = it->second.second;
+      S.tuning = "cached";
+    }
+  }
+  if (S.tuning.empty() && S.updates >= kTuneMinUpdates) {
+    cudaStream_t st;
+    TOMO_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    double2 *work = (double2 *)p.d_scratch;
+    int rc = TOMO_OK;
+    if (cudaMemsetAsync(p.d_scratch, 0, p.scratch_bytes, st) != cudaSuccess) rc = TOMO_ECUDA;
+    // the sinogram-row area (after all prefix lines) holds the packed sinograms,
+    // the prefix-line area the packed images
+    float *fwd_out = (float *)(work + S.inst[0].as);
+    float *adj_out = (float *)work;
+    std::string log;
+    for (int dir = 0; dir < 2 && rc == TOMO_OK; ++dir) {
+      float best = 1e30f;
+      log += dir == 0 ? "fwd" : "; adj";
+      for (int c = 0; c < kNumCfg && rc == TOMO_OK; ++c) {
+        int grid = 0;
+        if ((rc = dd_grid(c, dir == 0, &grid))) break;
+        float ms = 0.0f;
+        for (int rep = 0; rep < 3 && rc == TOMO_OK; ++rep) {
+          cudaEventRecord(e0, st);
+          rc = dir == 0 ? dd_launch_fwd(S, c, grid, work, fwd_out, st, FwdEpi())
+                        : dd_launch_adj(S, c, grid, work, adj_out, st, AdjEpi());
+          cudaEventRecord(e1, st);
+          cudaEventSynchronize(e1);
+          float t = 0.0f;
+          cudaEventElapsedTime(&t, e0, e1);
+          if (rep) ms += t;
+        }
+        char buf[48];
+        std::snprintf(buf, sizeof(buf), " %s=%.3fms", cfg_name(c).c_str(), ms / 2);
+        log += buf;
+        if (ms < best) {
+          best = ms;
+          (dir == 0 ? S.wf : S.wa) = c;
+        }
+      }
+    }
+    cudaError_t err = cudaStreamSynchronize(st);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaStreamDestroy(st);
+    if (rc) return rc;
+    if (err != cudaSuccess) return cuda_fail(err, "dd autotune");
+    S.tuning = "timed:" + log.substr(0);
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tuned[key] = std::make_pair(S.wf, S.wa);
+  }
+  if (S.tuning.empty()) S.tuning = "default (small workload)";
+  int rc = dd_grid(S.wf, true, &S.grid_f);
+  if (!rc) rc = dd_grid(S.wa, false, &S.grid_a);
+  S.tuning = "fwd " + cfg_name(S.wf) + ", adj " + cfg_name(S.wa) + " (w<warps/block> + b: block fetch, w: warp fetch)" +
+             ", grids " + std::to_string(S.grid_f) + "/" + std::to_string(S.grid_a) + " (" + S.tuning + ")";
+  return rc;
+}
+
+// One geometry of a plan or batch: n, angles and the number of slices.
+struct DdGeo {
+  int n, na, nz;
+  const float *angles;
+};
+
+// Builds the instance table, the device tables and the scratch of a plan
+// whose geometries are geo[0..count) (in the caller's packed order).
+int dd_build(Plan &p, const DdGeo *geo, int count) {
+  auto *S = new DdState();
+  p.ext = S;
+  p.ext_free = dd_state_free;
+  // host tables per geometry, packed into one device buffer
+  struct GeoTabs {
+    size_t ang, tab, tabS;
+    int nR, nC, nS, pads, w2;
+  };
+  std::vector<GeoTabs> gt(count);
+  std::vector<char> blob;
+  auto put = [&blob](const void *src, size_t bytes) {
+    const size_t off = (blob.size() + 15) / 16 * 16;
+    blob.resize(off + bytes);
+    if (bytes) std::memcpy(blob.data() + off, src, bytes);
+    return off;
+  };
+  for (int gi = 0; gi < count; ++gi) {
+    const DdGeo &G = geo[gi];
+    const int n = G.n, na = G.na, nh = (int)(n * 0.5);
+    std::vector<DdAngle> tab(na);
+    int rc = dd_build_table(G.angles, na, tab.data());
+    if (rc) return rc;
+    GeoTabs &t = gt[gi];
+    // detector boundaries of every pixel boundary of the image (and of a
+    // 4-pixel tile margin beyond it) lie within pads entries of [0, n)
+    t.pads = (int)std::ceil((nh + 1) * (std::sqrt(2.0) - 1.0)) + 12;
+    t.w2 = n + 2 * t.pads;
+    if ((double)na * t.w2 >= 2147483647.0) return fail(TOMO_EINVAL, "dd: nang * (npix + pads) too large");
+    std::vector<float4> rows, cols;
+    std::vector<int2> sums;
+    for (int v = 0; v < na; ++v) {
+      const DdAngle &a = tab[v];
+      const int off = v * t.w2;
+      if (a.mode == DD_ROWS || a.mode == DD_COLS) {
+        // z = 1/r (the sine or cosine): the detector of a boundary P is about P z + nh
+        float s, c;
+        sincosf(G.angles[v], &s, &c);
+        float4 e = make_float4(a.r, a.k, a.mode == DD_ROWS ? s : c, 0.0f);
+        std::memcpy(&e.w, &off, sizeof(int));
+        (a.mode == DD_ROWS ? rows : cols).push_back(e);
+      } else if (a.mode == DD_ROWSUM || a.mode == DD_COLSUM) {
+        sums.push_back(make_int2(a.mode, off));
+      }
+    }
+    t.nR = (int)rows.size();
+    t.nC = (int)cols.size();
+    t.nS = (int)sums.size();
+    rows.insert(rows.end(), cols.begin(), cols.end());
+    t.ang = put(tab.data(), sizeof(DdAngle) * na);
+    t.tab = put(rows.data(), sizeof(float4) * rows.size());
+    t.tabS = put(sums.data(), sizeof(int2) * sums.size());
+  }
+  TOMO_CUDA(cudaMalloc(&S->d_tables, std::max<size_t>(blob.size(), 16)));
+  TOMO_CUDA(cudaMemcpy(S->d_tables, blob.data(), blob.size(), cudaMemcpyHostToDevice));
+  const char *tb = (const char *)S->d_tables;
+  // instances in the caller's order, with packed offsets
+  std::vector<DdInst> inst;
+  std::vector<double> cost;
+  size_t io = 0, so = 0;
+  S->img_off.push_back(0);
+  S->sino_off.push_back(0);
+  for (int gi = 0; gi < count; ++gi) {
+    const DdGeo &G = geo[gi];
+    const GeoTabs &t = gt[gi];
+    for (int z = 0; z < G.nz; ++z) {
+      DdInst I{};
+      I.n = G.n;
+      I.nh = (int)(G.n * 0.5);
+      I.na = G.na;
+      I.pads = t.pads;
+      I.w2 = t.w2;
+      I.nR = t.nR;
+      I.nC = t.nC;
+      I.nS = t.nS;
+      I.ngrp = (G.n + kGrpDet - 1) / kGrpDet;
+      I.tx = (G.n + kTileW - 1) / kTileW;
+      I.ty = (G.n + kTileH - 1) / kTileH;
+      I.ang = (const DdAngle *)(tb + t.ang);
+      I.tab = (const float4 *)(tb + t.tab);
+      I.tabS = (const int2 *)(tb + t.tabS);
+      I.img = (long long)io;
+      I.sino = (long long)so;
+      io += (size_t)G.n * G.n;
+      so += (size_t)G.na * G.n;
+      S->img_off.push_back(io);
+      S->sino_off.push_back(so);
+      inst.push_back(I);
+      cost.push_back((double)G.n * G.n * G.na);
+      S->updates += (double)G.n * G.n * G.na;
+    }
+  }
+  // scheduling order: largest work first, caller's order among equals
+  std::vector<int> order(inst.size());
+  for (size_t i = 0; i < order.size(); ++i) order[i] = (int)i;
+  std::stable_sort(order.begin(), order.end(), [&cost](int a, int b) { return cost[a] > cost[b]; });
+  // scratch: every instance's prefix lines, then every instance's sinogram rows
+  size_t work = 0;
+  for (int idx : order) work += 2 * (size_t)inst[idx].n * (inst[idx].n + 2);
+  size_t sl_at = 0, as_at = work;
+  for (int idx : order) work += (size_t)inst[idx].na * inst[idx].w2;
+  for (int idx : order) {
+    DdInst I = inst[idx];
+    I.sl = (long long)sl_at;
+    sl_at += 2 * (size_t)I.n * (I.n + 2);
+    I.as = (long long)as_at;
+    as_at += (size_t)I.na * I.w2;
+    I.f0 = S->fwd_items;
+    S->fwd_items += (long long)I.na * I.ngrp;
+    I.a0 = S->adj_items;
+    S->adj_items += (long long)I.tx * I.ty;
+    I.r0 = S->row_blocks;
+    S->row_blocks += I.n;
+    I.c0 = S->col_blocks;
+    S->col_blocks += (I.n + 31) / 32;
+    I.s0 = S->sino_blocks;
+    S->sino_blocks += I.na;
+    S->inst.push_back(I);
+  }
+  if (S->row_blocks > 2147483647LL || S->sino_blocks > 2147483647LL)
+    return fail(TOMO_EINVAL, "dd: batch too large for one launch");
+  TOMO_CUDA(cudaMalloc(&S->d_inst, sizeof(DdInst) * S->inst.size()));
+  TOMO_CUDA(cudaMemcpy(S->d_inst, S->inst.data(), sizeof(DdInst) * S->inst.size(), cudaMemcpyHostToDevice));
+  TOMO_CUDA(cudaMalloc(&S->d_ctr, 2 * sizeof(unsigned long long)));
+  p.scratch_bytes = sizeof(double2) * work;
+  TOMO_CUDA(cudaMalloc(&p.d_scratch, p.scratch_bytes));
+  p.fwd_warps = (size_t)S->fwd_items;  // one residual partial per forward item
+  p.img_total = io;
+  p.sino_total = so;
+  return dd_autotune(p, *S);
+}
+
+}  // namespace
+
+int dd_setup(Plan &p) {
+  DdGeo G{p.g.n, p.g.na, p.g.nz, p.angles.data()};
+  return dd_build(p, &G, 1);
+}
+
+int dd_setup_batch(Plan &p, const tomo_geom *geoms, int count) {
+  std::vector<DdGeo> geo(count);
+  for (int i = 0; i < count; ++i) geo[i] = DdGeo{geoms[i].n, geoms[i].na, geoms[i].nz, geoms[i].angles};
+  return dd_build(p, geo.data(), count);
+}
+
+int dd_layout(const Plan &p, int *instances, size_t *img_off, size_t *sino_off, size_t cap) {
+  const DdState &S = *(const DdState *)p.ext;
+  const size_t ni = S.img_off.size() - 1;
+  if (instances) *instances = (int)ni;
+  if (img_off || sino_off) {
+    if (cap < ni + 1) return fail(TOMO_EINVAL, "layout: arrays need instances + 1 entries");
+    for (size_t i = 0; i <= ni; ++i) {
+      if (img_off) img_off[i] = S.img_off[i];
+      if (sino_off) sino_off[i] = S.sino_off[i];
+    }
+  }
+  return TOMO_OK;
+}
+
+const std::string &dd_tuning(const Plan &p) { return ((const DdState *)p.ext)->tuning; }
+
+int dd_forward(Plan &p, const float *d_img, float *d_sino, cudaStream_t s, const FwdEpi &ep) {
+  const DdState &S = *(const DdState *)p.ext;
+  double2 *work = (double2 *)p.d_scratch;
+  const int ni = (int)S.inst.size();
+  dd_row_prefix_kernel<<<(unsigned)S.row_blocks, kScanThreads, 0, s>>>(S.d_inst, ni, d_img, work);
+  dd_col_prefix_kernel<<<(unsigned)S.col_blocks, 32 * kColWarps, 0, s>>>(S.d_inst, ni, d_img, work);
+  TOMO_CUDA(cudaGetLastError());
+  return dd_launch_fwd(S, S.wf, S.grid_f, work, d_sino, s, ep);
 }
 
 int dd_adjoint(Plan &p, const float *d_sino, float *d_img, cudaStream_t s, const AdjEpi &ep) {
-  const int n = p.g.n, na = p.g.na, nz = p.g.nz;
-  float *Sp = p.d_scratch + 2 * (size_t)nz * n * p.dd_wl;
-  dim3 pb(256), pg((p.dd_w + 255) / 256, na, nz);
-  dd_pad_sino_kernel<<<pg, pb, 0, s>>>(d_sino, Sp, (const DdAngle *)p.d_angles, n, na, p.dd_w,
-                                       p.dd_pads);
-  const float4 *tR = (const float4 *)p.d_aux, *tC = tR + p.dd_nR;
-  const int2 *tS = (const int2 *)(tC + p.dd_nC);
-  dim3 ab(32, 8), ag((n + 63) / 64, (n + 15) / 16, nz);
-  dd_adjoint_v3_kernel<<<ag, ab, 0, s>>>(Sp, d_img, tR, p.dd_nR, tC, p.dd_nC, tS, p.dd_nS, n, p.nh,
-                                         na, p.dd_w, p.dd_pads, ep);
+  const DdState &S = *(const DdState *)p.ext;
+  double2 *work = (double2 *)p.d_scratch;
+  const int ni = (int)S.inst.size();
+  dd_sino_expand_kernel<<<(unsigned)S.sino_blocks, kScanThreads, 0, s>>>(S.d_inst, ni, d_sino, work);
   TOMO_CUDA(cudaGetLastError());
-  return TOMO_OK;
+  return dd_launch_adj(S, S.wa, S.grid_a, work, d_img, s, ep);
 }
 
 }  // namespace tomo

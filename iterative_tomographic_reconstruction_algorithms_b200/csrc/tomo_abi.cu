@@ -30,8 +30,8 @@ int cuda_fail(cudaError_t e, const char *what) {
   return TOMO_ECUDA;
 }
 
-size_t image_elems(const Plan &p) { return (size_t)p.g.nz * p.g.n * p.g.n; }
-size_t sino_elems(const Plan &p) { return (size_t)p.g.nz * p.g.na * p.g.n; }
+size_t image_elems(const Plan &p) { return p.img_total ? p.img_total : (size_t)p.g.nz * p.g.n * p.g.n; }
+size_t sino_elems(const Plan &p) { return p.sino_total ? p.sino_total : (size_t)p.g.nz * p.g.na * p.g.n; }
 
 static void release(Plan &p) {
   if (p.d_angles) cudaFree(p.d_angles);
@@ -148,6 +148,60 @@ int tomo_plan_create(const tomo_geom *geom, tomo_plan **out) {
   }
   if (!p.fwd_warps) p.fwd_warps = (size_t)((p.g.n + 127) / 128) * 4 * p.g.na * p.g.nz;
   *out = tp;
+  return TOMO_OK;
+}
+
+int tomo_plan_create_batch(const tomo_geom *geoms, int count, tomo_plan **out) {
+  if (!out) return fail(TOMO_EINVAL, "plan output pointer is NULL");
+  *out = nullptr;
+  if (!geoms || count < 1) return fail(TOMO_EINVAL, "batch: need at least one geometry");
+  size_t instances = 0;
+  for (int i = 0; i < count; ++i) {
+    int rc = validate(&geoms[i]);
+    if (rc) return fail(rc, "batch geometry " + std::to_string(i) + ": " + g_last_error);
+    if (geoms[i].kind != TOMO_KIND_DD)
+      return fail(TOMO_EINVAL, "batch geometry " + std::to_string(i) +
+                                   ": batched plans are available for the distance-driven pair only");
+    instances += (size_t)geoms[i].nz;
+  }
+  if (instances > (1u << 24)) return fail(TOMO_EINVAL, "batch: more than 2^24 instances");
+  auto *tp = new tomo_plan();
+  Plan &p = tp->p;
+  p.g = geoms[0];
+  p.g.angles = nullptr;
+  p.nh = (int)(p.g.n * 0.5);
+  cudaGetDevice(&p.device);
+  int rc = dd_setup_batch(p, geoms, count);
+  if (rc) {
+    release(p);
+    delete tp;
+    return rc;
+  }
+  *out = tp;
+  return TOMO_OK;
+}
+
+int tomo_plan_layout(tomo_plan *plan, int *instances, size_t *img_off, size_t *sino_off, size_t cap) {
+  if (!plan) return fail(TOMO_EINVAL, "layout: NULL plan");
+  const Plan &p = plan->p;
+  if (p.g.kind != TOMO_KIND_DD) {
+    if (instances) *instances = p.g.nz;
+    if (img_off || sino_off) {
+      if (cap < (size_t)p.g.nz + 1) return fail(TOMO_EINVAL, "layout: arrays need instances + 1 entries");
+      for (int z = 0; z <= p.g.nz; ++z) {
+        if (img_off) img_off[z] = (size_t)z * p.g.n * p.g.n;
+        if (sino_off) sino_off[z] = (size_t)z * p.g.na * p.g.n;
+      }
+    }
+    return TOMO_OK;
+  }
+  return dd_layout(p, instances, img_off, sino_off, cap);
+}
+
+int tomo_plan_tuning(tomo_plan *plan, char *buf, size_t len) {
+  if (!plan) return fail(TOMO_EINVAL, "tuning: NULL plan");
+  const std::string t = plan->p.g.kind == TOMO_KIND_DD ? dd_tuning(plan->p) : std::string("fixed launch shape");
+  if (buf && len) std::snprintf(buf, len, "%s", t.c_str());
   return TOMO_OK;
 }
 

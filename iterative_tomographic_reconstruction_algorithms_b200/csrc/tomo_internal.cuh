@@ -88,6 +88,9 @@ struct Plan {
   int dd_pads = 0, dd_w = 0, dd_wl = 0, dd_nR = 0, dd_nC = 0, dd_nS = 0;
   // warps of the forward launch that write residual partial sums (solver.cu)
   size_t fwd_warps = 0;
+  // packed image / sinogram sizes in floats when they are not nz*n*n and
+  // nz*na*n (batched plans of uneven geometries)
+  size_t img_total = 0, sino_total = 0;
   // kind-specific state owned by the plan (gridding), freed with ext_free
   void *ext = nullptr;
   void (*ext_free)(void *) = nullptr;
@@ -110,6 +113,12 @@ TOMO_DECLARE_KIND(rd)  // radon_rd.cu
 TOMO_DECLARE_KIND(bs)  // bspline.cu
 TOMO_DECLARE_KIND(grid)  // grid.cu
 #undef TOMO_DECLARE_KIND
+
+// Batched distance-driven plans (radon_dd.cu): geometries of different sizes
+// packed back to back, run by the same persistent kernels as a plan's slices.
+int dd_setup_batch(Plan &p, const tomo_geom *geoms, int count);
+int dd_layout(const Plan &p, int *instances, size_t *img_off, size_t *sino_off, size_t cap);
+const std::string &dd_tuning(const Plan &p);
 
 // Plan-less pieces of the dd forward (radon_dd.cu), used by dd_noalloc.cu.
 int dd_build_table(const float *angles, int na, DdAngle *tab);

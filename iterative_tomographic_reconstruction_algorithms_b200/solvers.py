@@ -48,11 +48,16 @@ class Solver:
         device = torch.device("cuda", torch.cuda.current_device()) if device is None else torch.device(device)
         self.device = device
         bd, _ = _as_device(b, torch, device)
-        if bd.dim() == 2:
-            bd = bd[None]
-        self.b = bd.contiguous()
-        self.nz = int(self.b.shape[0])
-        self.plan = tp.plan(self.nz, device.index)
+        if isinstance(tp, _lib.Plan):  # a plan (e.g. a batched plan over packed arrays)
+            self.plan = tp
+            self.b = bd.reshape(tp.sino_shape).contiguous()
+            self.nz = 0
+        else:
+            if bd.dim() == 2:
+                bd = bd[None]
+            self.b = bd.contiguous()
+            self.nz = int(self.b.shape[0])
+            self.plan = tp.plan(self.nz, device.index)
         h = ctypes.c_void_p()
         stream = torch.cuda.current_stream(device).cuda_stream
         _lib.check(_lib.lib.tomo_solver_create(self.plan._h, ALGOS[algo], self.b.data_ptr(), stream,
@@ -63,13 +68,18 @@ class Solver:
         """Run ``iters`` iterations from ``x`` (numpy or CUDA tensor); returns (x, residuals)."""
         torch = self.torch
         xd, was_np = _as_device(x, torch, self.device)
-        squeeze = xd.dim() == 2
+        in_shape = tuple(xd.shape)
+        squeeze = self.nz > 0 and xd.dim() == 2
         xd = (xd[None] if squeeze else xd).clone()
+        if self.nz == 0:
+            xd = xd.reshape(self.plan.image_shape)
         res = (ctypes.c_double * max(iters, 1))()
         stream = torch.cuda.current_stream(self.device).cuda_stream
         _lib.check(_lib.lib.tomo_solver_run(self._h, xd.data_ptr(), int(iters), res, int(use_graph), stream),
                    "tomo_solver_run")
         out = xd[0] if squeeze else xd
+        if self.nz == 0:
+            out = out.reshape(in_shape)
         if was_np:
             out = out.cpu().numpy()
         return out, np.array(res[:iters])
