@@ -39,6 +39,20 @@ def test_library_exports_every_declared_symbol():
     assert not missing, f"declared in {HEADER.name} but not exported: {missing}"
 
 
+def test_nn_library_exports_every_declared_symbol():
+    header = ROOT / "include" / "tomo_nn.h"
+    lib = ROOT / "iterative_tomographic_reconstruction_algorithms_b200" / "libtomo_nn.so"
+    assert lib.exists(), "build libtomo_nn.so first (make -C iterative_tomographic_reconstruction_algorithms_b200/csrc)"
+    text = re.sub(r"/\*.*?\*/", "", header.read_text(), flags=re.S)
+    declared = sorted(set(re.findall(r"\b(tomo_nn_[a-z0-9_]+)\s*\(", text)))
+    assert "tomo_nn_conv3x3" in declared and "tomo_nn_wgrad" in declared
+    out = subprocess.run(["nm", "-D", "--defined-only", str(lib)], capture_output=True, text=True,
+                         check=True).stdout
+    exported = {line.split()[-1] for line in out.splitlines() if line.strip()}
+    missing = [s for s in declared if s not in exported]
+    assert not missing, f"declared in {header.name} but not exported: {missing}"
+
+
 def test_library_loads_and_reports_version():
     from iterative_tomographic_reconstruction_algorithms_b200 import _lib
     assert b"sm_100a" in _lib.lib.tomo_version()
