@@ -202,10 +202,14 @@ class UNet(torch.nn.Module):
         self.head_w = torch.nn.Parameter(torch.zeros((8, cin)))
         self.head_b = torch.nn.Parameter(torch.zeros(8))
 
-    def forward(self, x):
+    def forward(self, x, extra=None):
+        """``extra``: optional further input channels, FP32 [B, H, W] or [B, H, W, k] (k <= 7)."""
         B, H, W = x.shape
         h = torch.zeros((B, H, W, self.CIN), dtype=torch.bfloat16, device=x.device)
         h[..., 0] = x.to(torch.bfloat16)
+        if extra is not None:
+            e = extra if extra.dim() == 4 else extra[..., None]
+            h[..., 1:1 + e.shape[-1]] = e.to(torch.bfloat16)
         skips = []
         first = True
         for lvl in range(self.levels):
