@@ -58,7 +58,7 @@ def parse():
     ap.add_argument("--train-pairs", type=int, default=256, help="warmstart: training samples")
     ap.add_argument("--train-steps", type=int, default=2000, help="warmstart: training steps")
     ap.add_argument("--eval-slices", type=int, default=16, help="warmstart: held-out slices")
-    ap.add_argument("--lam", type=float, default=1.0, help="warmstart: weight of the data-consistency loss")
+    ap.add_argument("--lam", type=float, default=0.03, help="warmstart: weight of the data-consistency loss")
     ap.add_argument("--slices", type=int, default=64, help="batch workload: number of slices")
     ap.add_argument("--iters", type=int, default=10, help="batch workload: SIRT iterations per step")
     return ap.parse_args()

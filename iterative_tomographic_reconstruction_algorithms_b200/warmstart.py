@@ -102,7 +102,7 @@ def apply_net(net, pb: Problem, x2, fb):
 
 
 def train(net, pb: Problem, data, steps: int = 1000, batch: int = 4, lr: float = 1e-3,
-          lam: float = 1.0, unroll: int = 5, seed: int = 0, log_every: int = 100):
+          lam: float = 0.03, unroll: int = 5, seed: int = 0, log_every: int = 100):
     """Trains ``net`` in place on ``make_pairs`` data; returns the loss history
     (one value per ``log_every`` steps).  The learning rate decays by cosine."""
     tp = projectors(pb.n_op, np.linspace(0, 180, pb.na, endpoint=False), oper="dd")
