@@ -33,11 +33,11 @@
 //
 // Work is described by a table of instances (one per slice, or per geometry
 // of an uneven batch) and consumed by persistent kernels: each warp takes the
-// next work item (forward: 127 detectors of one angle; adjoint: a 32x16 pixel
+// next work item (forward: 127 detectors of one angle; adjoint: a 16x8 pixel
 // tile over all angles) from a device counter, finds its instance by binary
 // search and runs it.  Every output element is owned by one lane and its sum
 // order is fixed, so results do not depend on scheduling and are
-// deterministic.  Warps per block are chosen per plan by timing the
+// deterministic.  Warps per block and the fetch mode are chosen per plan by timing the
 // candidates (dd_autotune).  The projection arithmetic of the solvers
 // (epilogue.cuh) is applied where the result is stored.
 #include <algorithm>
