@@ -27,8 +27,8 @@
 //            P_j+1 - P_j in float, i.e. 1 to within an ulp of P.
 //   adjoint  a pixel is at most one detector wide (r >= 1), so it overlaps the
 //            detector holding its left boundary and possibly the next: two
-//            float gaps, as the reference forms them, from one table entry
-//            {D_a, S_a, D_a+1, S_a+1} per angle.
+//            float gaps, as the reference forms them, from one 8-byte table
+//            entry {S_a, S_a+1} per angle and the boundary D_a+1 recomputed.
 // The dropped last piece is subtracted where it falls (dd_dropped_piece).
 //
 // Work is described by a table of instances (one per slice, or per geometry
@@ -327,9 +327,9 @@ __global__ void __launch_bounds__(32 * kColWarps) dd_col_prefix_kernel(const DdI
 }
 
 // Sinogram rows, one block per angle v: entry e = m + pads (m in
-// [-pads, n + pads)) holds {D_m, S_m, D_m+1, S_m+1}, the detector boundaries
-// and values (S = 0 outside [0, n)) that a pixel starting in detector m
-// overlaps.  Row / column-sum angles only use S_m.
+// [-pads, n + pads)) holds {S_m, S_m+1}, the values (0 outside [0, n)) of the
+// two detectors a pixel starting in detector m can overlap.  (The boundary
+// D_m+1 between them is recomputed from m where it is needed.)
 __global__ void __launch_bounds__(kScanThreads) dd_sino_expand_kernel(const DdInst *__restrict__ inst,
                                                                       int ninst, const float *__restrict__ sino,
                                                                       double2 *__restrict__ work) {
@@ -338,14 +338,13 @@ __global__ void __launch_bounds__(kScanThreads) dd_sino_expand_kernel(const DdIn
   const int v = (int)(b - I.s0), n = I.n, nh = I.nh, pads = I.pads, w2 = I.w2;
   const DdAngle g = I.ang[v];
   const float *src = sino + I.sino + (size_t)g.out_row * n;
-  float4 *dst = (float4 *)(work + I.as) + (size_t)v * w2;
-  const bool lines = g.mode == DD_ROWS || g.mode == DD_COLS;
+  float2 *dst = (float2 *)(work + I.as) + (size_t)v * w2;
+  (void)nh;
   for (int e = threadIdx.x; e < w2; e += blockDim.x) {
     const int m = e - pads;
     const float s0 = (m >= 0 && m < n) ? __ldg(src + m) : 0.0f;
     const float s1 = (m + 1 >= 0 && m + 1 < n) ? __ldg(src + m + 1) : 0.0f;
-    dst[e] = lines ? make_float4(det_bound(m, nh, g.r), s0, det_bound(m + 1, nh, g.r), s1)
-                   : make_float4(0.0f, s0, 0.0f, s1);
+    dst[e] = make_float2(s0, s1);
   }
 }
 
@@ -506,20 +505,22 @@ __global__ void __launch_bounds__(32 * W) dd_fwd_kernel(const DdInst *__restrict
 // one pixel wide): (min(D_a+1, P1) - P0) S_a + (P1 - min(D_a+1, P1)) S_a+1,
 // the reference's two gaps.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ float dd_adj_pixel(float P0, float P1, float z, float cm,
-                                              const float4 *__restrict__ rowm) {
-  // a = floor(P0 z + nh) by rounding at 1.5 * 2^23, read as the float's bits
-  // (rowm is the row base minus kMagicBits entries); one off at a detector
-  // boundary only moves a zero-width piece
-  const float4 t = __ldg(rowm + __float_as_int(__fadd_rn(__fmaf_rn(P0, z, -0.5f), cm)));
-  // t = {D_a, S_a, D_a+1, S_a+1}
-  const float m = fminf(t.z, P1);
-  return fmaf(__fsub_rn(P1, m), t.w, __fmul_rn(__fsub_rn(m, P0), t.y));
+__device__ __forceinline__ float dd_adj_pixel(float P0, float P1, float z, float r, float cm,
+                                              const float2 *__restrict__ rowm) {
+  // a = floor(P0 z + nh) by rounding at 1.5 * 2^23 (f = kMagic + a), read as
+  // the float's bits (rowm is the row base minus kMagicBits entries); one off
+  // at a detector boundary only moves a zero-width piece
+  const float f = __fadd_rn(__fmaf_rn(P0, z, -0.5f), cm);
+  const float2 t = __ldg(rowm + __float_as_int(f));  // {S_a, S_a+1}
+  // D_a+1 = (a + 1 - nh) r, with a + 1 - nh = f - (kMagic + nh - 1) exactly
+  const float D1 = __fmul_rn(__fsub_rn(f, __fsub_rn(cm, 1.0f)), r);
+  const float m = fminf(D1, P1);
+  return fmaf(__fsub_rn(P1, m), t.y, __fmul_rn(__fsub_rn(m, P0), t.x));
 }
 
 template <bool COLS>
 __device__ __forceinline__ void dd_adj_pass(const float4 *__restrict__ tab, int cnt,
-                                            const float4 *__restrict__ AS, int a0, int b0, int n, int nh,
+                                            const float2 *__restrict__ AS, int a0, int b0, int n, int nh,
                                             float (&acc)[2][2]) {
   const int l0 = COLS ? b0 : a0, k0 = COLS ? a0 : b0;
   const float y0 = (float)(l0 - nh) + 0.5f, y1 = __fadd_rn(y0, 1.0f);
@@ -530,18 +531,18 @@ __device__ __forceinline__ void dd_adj_pass(const float4 *__restrict__ tab, int 
   for (int u = 0; u < cnt; ++u) {
     const float4 e = __ldg(tab + u);
     const float r = e.x, k = e.y, z = e.z;
-    const float4 *row = AS + __float_as_int(e.w);
-    const float4 *rowm = row - kMagicBits;
+    const float2 *row = AS + __float_as_int(e.w);
+    const float2 *rowm = row - kMagicBits;
     const float Dn = det_bound(n, nh, r);
 #pragma unroll
     for (int li = 0; li < 2; ++li) {
       const float q = __fmul_rn(li ? y1 : y0, k);
       const float P0 = __fsub_rn(x0, q), P1 = __fsub_rn(x1, q), P2 = __fsub_rn(x2, q);
-      float s0 = dd_adj_pixel(P0, P1, z, cm, rowm), s1 = dd_adj_pixel(P1, P2, z, cm, rowm);
+      float s0 = dd_adj_pixel(P0, P1, z, r, cm, rowm), s1 = dd_adj_pixel(P1, P2, z, r, cm, rowm);
       if (lastpix || (P0 < Dn && Dn < P2)) {
         DdDrop d;
         if (dd_dropped_piece(q, r, n, nh, d)) {
-          const float sd = __fmul_rn(d.gap, __ldg(&row[d.det].y));
+          const float sd = __fmul_rn(d.gap, __ldg(&row[d.det].x));
           if (d.pix == k0) s0 -= sd;
           else if (d.pix == k0 + 1) s1 -= sd;
         }
@@ -563,7 +564,7 @@ __device__ __forceinline__ void dd_adj_item(const DdInst &I, int txi, int tyi, i
   const int n = I.n, nh = I.nh;
   const int b0 = txi * kTileW + 2 * (lane & 7), a0 = tyi * kTileH + 2 * (lane >> 3);
   float acc[2][2] = {{0.0f, 0.0f}, {0.0f, 0.0f}};
-  const float4 *AS = (const float4 *)(work + I.as) + I.pads;
+  const float2 *AS = (const float2 *)(work + I.as) + I.pads;
   // tiles that start outside the image (n not a multiple of the tile) only
   // take part in the epilogue's warp reductions
   const bool inside = a0 < n && b0 < n;
@@ -573,11 +574,11 @@ __device__ __forceinline__ void dd_adj_item(const DdInst &I, int txi, int tyi, i
   }
   for (int t = 0; inside && t < I.nS; ++t) {  // row / column sums (|sin| or |cos| < 1e-7)
     const int2 e = __ldg(I.tabS + t);
-    const float4 *row = AS + e.y;
+    const float2 *row = AS + e.y;
 #pragma unroll
     for (int i = 0; i < 2; ++i)
 #pragma unroll
-      for (int j = 0; j < 2; ++j) acc[i][j] += __ldg(&row[e.x == DD_ROWSUM ? a0 + i : b0 + j].y);
+      for (int j = 0; j < 2; ++j) acc[i][j] += __ldg(&row[e.x == DD_ROWSUM ? a0 + i : b0 + j].x);
   }
 #pragma unroll
   for (int i = 0; i < 2; ++i)
