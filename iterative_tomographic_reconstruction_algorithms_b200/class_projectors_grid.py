@@ -89,7 +89,7 @@ class projectors:
 
     def _apply(self, x, forward: bool, which: str):
         if isinstance(x, np.ndarray) or not hasattr(x, "is_cuda"):
-            x = np.asarray(x).astype(myfloat)
+            x = np.ascontiguousarray(x, dtype=myfloat)  # no copy when already float32 (inputs are never modified)
             device = None
         else:
             device = x.device.index

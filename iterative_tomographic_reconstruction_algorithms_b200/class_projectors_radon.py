@@ -81,7 +81,7 @@ class projectors:
     def _apply(self, x, forward: bool):
         is_np = isinstance(x, np.ndarray) or not hasattr(x, "is_cuda")
         if is_np:
-            x = np.asarray(x).astype(myfloat)
+            x = np.ascontiguousarray(x, dtype=myfloat)  # no copy when already float32 (inputs are never modified)
             device = None
         else:
             device = x.device.index

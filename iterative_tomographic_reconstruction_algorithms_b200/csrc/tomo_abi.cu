@@ -10,6 +10,9 @@
 #include <string>
 #include <tuple>
 #include <vector>
+#include <thread>
+#include <atomic>
+#include <algorithm>
 
 #include "tomo_internal.cuh"
 
@@ -40,6 +43,10 @@ static void release(Plan &p) {
   if (p.d_in) cudaFree(p.d_in);
   if (p.d_out) cudaFree(p.d_out);
   if (p.host_stream) cudaStreamDestroy(p.host_stream);
+  if (p.h_stage) cudaFreeHost(p.h_stage);
+  for (cudaEvent_t e : p.stage_events) cudaEventDestroy(e);
+  p.stage_events.clear();
+  p.h_stage = nullptr;
   if (p.ext && p.ext_free) p.ext_free(p.ext);
   p.ext = nullptr;
   p.d_angles = p.d_aux = nullptr;
@@ -225,14 +232,91 @@ int tomo_adjoint(tomo_plan *plan, const float *d_sino, float *d_image, void *str
 static int ensure_host_buffers(Plan &p) {
   if (!p.host_stream) TOMO_CUDA(cudaStreamCreateWithFlags(&p.host_stream, cudaStreamNonBlocking));
   const size_t ib = sizeof(float) * image_elems(p), sb = sizeof(float) * sino_elems(p);
+  const size_t mb = ib > sb ? ib : sb;
   if (!p.d_in) {
-    TOMO_CUDA(cudaMalloc(&p.d_in, ib > sb ? ib : sb));
-    p.d_in_bytes = ib > sb ? ib : sb;
+    TOMO_CUDA(cudaMalloc(&p.d_in, mb));
+    p.d_in_bytes = mb;
   }
   if (!p.d_out) {
-    TOMO_CUDA(cudaMalloc(&p.d_out, ib > sb ? ib : sb));
-    p.d_out_bytes = ib > sb ? ib : sb;
+    TOMO_CUDA(cudaMalloc(&p.d_out, mb));
+    p.d_out_bytes = mb;
   }
+  if (!p.h_stage) {
+    // pinned staging; if the system refuses pinned memory the copies go
+    // straight from the caller's (pageable) arrays instead
+    if (cudaMallocHost(&p.h_stage, mb) == cudaSuccess) p.h_stage_bytes = mb;
+    else {
+      cudaGetLastError();
+      p.h_stage = nullptr;
+    }
+  }
+  return TOMO_OK;
+}
+
+// Host <-> device copies through the pinned staging buffer, in chunks: several
+// host threads copy chunks between the caller's array and the staging buffer,
+// and each chunk's DMA is queued as soon as its host copy is done (and the
+// host copy of an output chunk starts as soon as its DMA has landed), so the
+// memcpy and the transfer overlap.
+constexpr size_t kStageChunk = (size_t)4 << 20;
+
+static int stage_threads(size_t bytes) {
+  const unsigned hc = std::thread::hardware_concurrency();
+  const size_t by_size = (bytes + kStageChunk - 1) / kStageChunk;
+  return (int)std::max<size_t>(1, std::min<size_t>({(size_t)8, (size_t)(hc ? hc / 2 : 1), by_size}));
+}
+
+static int stage_in(Plan &p, const void *src, void *dst, size_t bytes) {
+  const size_t nch = (bytes + kStageChunk - 1) / kStageChunk;
+  const int nt = stage_threads(bytes);
+  std::atomic<int> err{0};
+  auto work = [&](int t) {
+    for (size_t c = (size_t)t; c < nch; c += (size_t)nt) {
+      const size_t off = c * kStageChunk, len = std::min(kStageChunk, bytes - off);
+      std::memcpy(p.h_stage + off, (const char *)src + off, len);
+      if (cudaMemcpyAsync((char *)dst + off, p.h_stage + off, len, cudaMemcpyHostToDevice, p.host_stream) !=
+          cudaSuccess)
+        err = 1;
+    }
+  };
+  std::vector<std::thread> th;
+  for (int t = 1; t < nt; ++t) th.emplace_back(work, t);
+  work(0);
+  for (auto &x : th) x.join();
+  if (err) return cuda_fail(cudaGetLastError(), "staged host-to-device copy");
+  return TOMO_OK;
+}
+
+static int stage_out(Plan &p, const void *src, void *dst, size_t bytes) {
+  const size_t nch = (bytes + kStageChunk - 1) / kStageChunk;
+  while (p.stage_events.size() < nch) {
+    cudaEvent_t e;
+    TOMO_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    p.stage_events.push_back(e);
+  }
+  for (size_t c = 0; c < nch; ++c) {
+    const size_t off = c * kStageChunk, len = std::min(kStageChunk, bytes - off);
+    TOMO_CUDA(cudaMemcpyAsync(p.h_stage + off, (const char *)src + off, len, cudaMemcpyDeviceToHost,
+                              p.host_stream));
+    TOMO_CUDA(cudaEventRecord(p.stage_events[c], p.host_stream));
+  }
+  const int nt = stage_threads(bytes);
+  std::atomic<int> err{0};
+  auto work = [&](int t) {
+    for (size_t c = (size_t)t; c < nch; c += (size_t)nt) {
+      const size_t off = c * kStageChunk, len = std::min(kStageChunk, bytes - off);
+      if (cudaEventSynchronize(p.stage_events[c]) != cudaSuccess) {
+        err = 1;
+        continue;
+      }
+      std::memcpy((char *)dst + off, p.h_stage + off, len);
+    }
+  };
+  std::vector<std::thread> th;
+  for (int t = 1; t < nt; ++t) th.emplace_back(work, t);
+  work(0);
+  for (auto &x : th) x.join();
+  if (err) return cuda_fail(cudaGetLastError(), "staged device-to-host copy");
   return TOMO_OK;
 }
 
@@ -243,11 +327,18 @@ static int host_call(tomo_plan *plan, const float *h_in, float *h_out, bool forw
   if (rc) return rc;
   const size_t ib = sizeof(float) * image_elems(p), sb = sizeof(float) * sino_elems(p);
   const size_t in_b = forward ? ib : sb, out_b = forward ? sb : ib;
-  TOMO_CUDA(cudaMemcpyAsync(p.d_in, h_in, in_b, cudaMemcpyHostToDevice, p.host_stream));
+  if (p.h_stage) rc = stage_in(p, h_in, p.d_in, in_b);
+  else TOMO_CUDA(cudaMemcpyAsync(p.d_in, h_in, in_b, cudaMemcpyHostToDevice, p.host_stream));
+  if (rc) return rc;
   rc = forward ? tomo_forward(plan, p.d_in, p.d_out, p.host_stream)
                : tomo_adjoint(plan, p.d_in, p.d_out, p.host_stream);
   if (rc) return rc;
-  TOMO_CUDA(cudaMemcpyAsync(h_out, p.d_out, out_b, cudaMemcpyDeviceToHost, p.host_stream));
+  if (p.h_stage) {
+    rc = stage_out(p, p.d_out, h_out, out_b);
+    if (rc) return rc;
+  } else {
+    TOMO_CUDA(cudaMemcpyAsync(h_out, p.d_out, out_b, cudaMemcpyDeviceToHost, p.host_stream));
+  }
   TOMO_CUDA(cudaStreamSynchronize(p.host_stream));
   return TOMO_OK;
 }

@@ -82,6 +82,10 @@ struct Plan {
   // host-call staging
   float *d_in = nullptr, *d_out = nullptr;  // device buffers for *_host calls
   size_t d_in_bytes = 0, d_out_bytes = 0;
+  // pinned staging for host calls (copies overlap their DMA chunk by chunk)
+  char *h_stage = nullptr;
+  size_t h_stage_bytes = 0;
+  std::vector<cudaEvent_t> stage_events;
   cudaStream_t host_stream = nullptr;
   int device = 0;
   // distance-driven layout (radon_dd.cu)
