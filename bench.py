@@ -37,7 +37,7 @@ WORKLOAD = "distance-driven pair, 2048x2048 image, 1800 angles [0,180), 2048 bin
 TAU_DD = 2  # gathered operand values per update (distance-driven)
 # DRAM bytes per launch of the two main kernels at 2048^2 x 1800, from one ncu capture
 # (dram__bytes_read.sum + dram__bytes_write.sum)
-DRAM_BYTES_PER_LAUNCH = {"forward": 520.77e6 + 18.58e6, "adjoint": 79.04e6 + 8.62e6}
+DRAM_BYTES_PER_LAUNCH = {"forward": 520.66e6 + 19.07e6, "adjoint": 37.88e6 + 0.0192e6}
 
 
 def parse():
