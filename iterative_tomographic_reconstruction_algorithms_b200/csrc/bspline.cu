@@ -52,6 +52,9 @@ __global__ void __launch_bounds__(128) bs_forward_kernel(
   const bool by_rows = fabsf(C) >= fabsf(S);  // along a row ps moves by C per pixel
   // taps reach bin b when b <= ps + s + mid < b + 1 (b = 0 also takes (-1, 0))
   const float plo = (float)(b - k.ds - 2) - k.fmid, phi = (float)(b + k.ds + 2) - k.fmid;
+  const bool even = (n & 1) == 0 && n >= 4;  // n = 2: the bin-0 boundary sits at 0, use the double rule
+  const float bm = (float)b - k.fmid, fds = (float)k.ds;  // b - n/2 (exact for even n)
+  const float b0lo = -k.fmid - 1.0f, b0hi = -k.fmid + 1.0f;
   float acc = 0.0f;
   for (int line = 0; line < (live ? n : 0); ++line) {
     // by rows: ky fixed, ps = kx*C + S*ky; by columns: kx fixed, ps = ky*S + kx*C
@@ -74,8 +77,37 @@ __global__ void __launch_bounds__(128) bs_forward_kernel(
       const int kyi = by_rows ? line : j, kxi = by_rows ? j : line;
       const float ky = (float)(-kyi + k.mid), kx = (float)(kxi - k.mid);
       const float ps = __fmaf_rn(kx, C, __fmul_rn(S, ky));
+      // the tap that lands in bin b: s0 = b - floor(ps + n/2), or a neighbour
+      // of it where the rounding of s + ps crosses an integer (or, for bin 0,
+      // where truncation folds (-1, 0) onto 0); each is checked with the exact
+      // bin rule, so the set of taps is the reference's
+      if (even) {
+        // n/2 is an integer: trunc((double)fl(s + ps) + n/2) == b reduces to
+        // floor(fl(s + ps)) == b - n/2 for b >= 1 and to fl(s + ps) in
+        // (-n/2 - 1, -n/2 + 1) for b = 0, exact in float (checked against the
+        // double rule on CPU for n = 4..4096, including floats next to integers)
+        const float s0 = __fsub_rn(bm, floorf(ps));
+        const float slo = fmaxf(__fsub_rn(s0, b == 0 ? 2.0f : 1.0f), -fds), shi = fminf(__fadd_rn(s0, 1.0f), fds);
+        if (slo > shi) continue;
+        const float val = __ldg(I + (size_t)kyi * n + kxi);
+        for (float sf = slo; sf <= shi; sf = __fadd_rn(sf, 1.0f)) {
+          const float t = __fadd_rn(sf, ps);
+          // (b = n/2: a tiny negative t rounds up to n/2 in the double sum)
+          const bool hit = b == 0 ? (t > b0lo && t < b0hi)
+                                  : (floorf(t) == bm ||
+                                     (bm == 0.0f && t < 0.0f && (int)__dadd_rn((double)t, k.mid) == b));
+          if (!hit) continue;
+          const int li = bs_lut(b, ps, k);
+          if (li >= k.lut_max || li < 0) continue;
+          acc = fmaf(__ldg(L + li), val, acc);
+        }
+        continue;
+      }
+      const int s0 = b - (int)floor(__dadd_rn((double)ps, k.mid));
+      const int slo = max(s0 - (b == 0 ? 2 : 1), -k.ds), shi = min(s0 + 1, k.ds);
+      if (slo > shi) continue;
       const float val = __ldg(I + (size_t)kyi * n + kxi);
-      for (int s = -k.ds; s <= k.ds; ++s) {
+      for (int s = slo; s <= shi; ++s) {
         const int yi = bs_bin(s, ps, k.mid);
         if (yi != b) continue;
         const int li = bs_lut(yi, ps, k);
