@@ -153,6 +153,28 @@ int tomo_solver_destroy(tomo_solver *solver);
 int tomo_radon_dd_forward_noalloc(const float *d_image, int npix, const float *angles, int nang,
                                   int nz, float *d_sino, void *stream);
 
+/* ---- sinogram pre-processing on the device (common/myimage/my_image_process.py) ---- */
+
+/* sino_edge_padding (my_image_process.py:142-157): d_out [nang][npix + 2*npad]
+ * = npad copies of column 0, the sinogram, npad copies of column npix-1. */
+int tomo_sino_edge_pad(const float *d_sino, int nang, int npix, int npad, float *d_out, void *stream);
+
+/* sino_correct_rot_axis (my_image_process.py:87-117): d_out [nang][npix] = each
+ * row shifted by ctr - npix/2.  Integer shifts: the reference's roll with the
+ * wrapped columns replaced by the edge column (exact).  Fractional shifts: Keys
+ * cubic convolution of the zero-extended row, where the reference uses scipy's
+ * 2-D Clough-Tocher griddata (the two agree to ~1e-3 of the signal on smooth
+ * data).  d_out must not alias d_sino. */
+int tomo_sino_center(const float *d_sino, int nang, int npix, double ctr, float *d_out, void *stream);
+
+/* ---- ADMM-TV / CG finite differences on the device (algorithms/cg.py:62-71) ---- */
+
+/* G: numpy.gradient of d_m [n0][n1] (float32): d_g0 along axis 0, d_g1 along axis 1. */
+int tomo_grad2d(const float *d_m, int n0, int n1, float *d_g0, float *d_g1, void *stream);
+/* Gt: d_out [n0][n1] (float64) = g1 . Gx + Gy . g0 with Gx, Gy the gradient matrices of
+ * identities, as the reference multiplies them densely; the same float64 numbers, O(n^2). */
+int tomo_grad2d_adjoint(const float *d_g0, const float *d_g1, int n0, int n1, double *d_out, void *stream);
+
 /* ---- drop-in entry points (reference C signatures; host pointers) ---- */
 
 /* radon_pd.c:20 `void radon_pd(float* image, int npix, float* angles, int nang,
