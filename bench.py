@@ -52,7 +52,7 @@ def parse():
                     help="run only warm-up + steps of the device path (for ncu captures)")
     ap.add_argument("--n", type=int, default=N_SIDE, help="image side (profiling only)")
     ap.add_argument("--na", type=int, default=N_ANG, help="angle count (profiling only)")
-    ap.add_argument("--workload", default="pair", choices=["pair", "batch", "warmstart"],
+    ap.add_argument("--workload", default="pair", choices=["pair", "batch", "warmstart", "admm"],
                     help="pair: the dd pair at 2048^2 x 1800 (default); batch: batched uneven SIRT; "
                          "warmstart: learned warm start, time to the plain SIRT residual")
     ap.add_argument("--train-pairs", type=int, default=256, help="warmstart: training samples")
@@ -60,6 +60,7 @@ def parse():
     ap.add_argument("--eval-slices", type=int, default=16, help="warmstart: held-out slices")
     ap.add_argument("--lam", type=float, default=0.03, help="warmstart: weight of the data-consistency loss")
     ap.add_argument("--slices", type=int, default=64, help="batch workload: number of slices")
+    ap.add_argument("--no-cpu-baseline", action="store_true", help="admm workload: skip the host reference sample")
     ap.add_argument("--iters", type=int, default=10, help="batch workload: SIRT iterations per step")
     return ap.parse_args()
 
@@ -293,6 +294,109 @@ def run_warmstart(args, rank, world, local):
             "pairs_s": t_pairs, "train_s": t_train, "loss_history": hist}), flush=True)
 
 
+def run_admm(args, rank, world, local):
+    """ADMM-TV (admm.lasso_tv) with the gridding pair: 1024^2 phantom centred in
+    1536 bins, 1500 angles on [0, 180), Kaiser-Bessel W = 6, oversampling 2
+    (4096^2 Fourier grid), linear interpolation, b = A x + Gaussian noise of
+    sigma 0.01 max(b) (seed 2), lambd1 = 0.1, lambd2 = 1, mu = 20, 5 inner CG
+    iterations.  A step is one ADMM outer iteration (6 projector pairs, the
+    Gt(G) stencils, shrinkage and multiplier update; one CUDA graph).  Metric:
+    outer iterations per second.  The working set (about 0.26 GB with the
+    Fourier grid) exceeds L2, so no flush is needed between steps."""
+    import torch
+    from iterative_tomographic_reconstruction_algorithms_b200 import admm as ad
+    from iterative_tomographic_reconstruction_algorithms_b200 import class_projectors_grid as cpg
+    from iterative_tomographic_reconstruction_algorithms_b200.phantom import embed, random_ellipses
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    n, na, side = 1536, 1500, 1024
+    deg = np.linspace(0, 180, na, endpoint=False)
+    tp = cpg.projectors(n, deg, kernel="kb", oversampl=2.0, W=6.0, errs=1e-3, interp="lin", verbose=False)
+    x_true = torch.from_numpy(embed(random_ellipses(side, seed=2), n)).to(dev)
+    b = tp.A(x_true)
+    g = torch.Generator(device=dev).manual_seed(2)
+    b = (b + 0.01 * float(b.max()) * torch.randn(b.shape, generator=g, device=dev)).contiguous()
+    l1, l2, mu, n2 = 0.1, 1.0, 20.0, 5
+    solver = ad.AdmmSolver(tp, "lasso-tv", b, l1, l2, mu, n2)
+    x = torch.ones((1, n, n), device=dev)
+    solver.run(x, max(1, args.warmup), reset=True)
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    stream = torch.cuda.current_stream(dev)
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        st = solver.run(x, args.steps, reset=False)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    # the projector pairs alone (6 per outer iteration), same stream
+    plan = tp.plan(1, dev.index)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    sino = plan.forward(x)
+    e0.record(stream)
+    for _ in range(6):
+        sino = plan.forward(x)
+        img = plan.adjoint(sino)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    pairs_ms = e0.elapsed_time(e1)
+    # end to end through the public API: host x and b in, host x out, track=False
+    xh = np.ones((1, n, n), np.float32)
+    bh = b.cpu().numpy()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ad.lasso_tv(xh, bh, tp, ad.Param(lambd1=l1, lambd2=l2, mu=mu, n_iter=args.steps, n_iter_pcg=n2), track=False)
+    torch.cuda.synchronize()
+    e2e_ms = (time.perf_counter() - t0) * 1e3 / args.steps
+    rel = float((x[0].double() - x_true.double()).norm() / x_true.double().norm())
+    cpu = None
+    if not args.no_cpu_baseline:
+        cpu = admm_cpu_baseline(tp, b[0].cpu().numpy(), n, n2)
+    upd = 12.0 * n * n * na  # 6 pairs of n^2 na updates per outer iteration
+    out = {
+        "metric": "ADMM-TV outer iterations per second (gridding pair, 5 inner CG iterations)",
+        "value": 1e3 / ms, "unit": "iterations/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f64 CG r, p)",
+        "data": "synthetic",
+        "config": {"workload": "ADMM-TV, 1024^2 phantom in 1536 bins, 1500 angles, gridding KB W=6 os=2 lin, "
+                               "sigma=0.01 max b, lambd1=0.1 lambd2=1 mu=20, 5 inner CG",
+                   "l2": "working set > L2, no flush"},
+        "projector_pairs_ms_per_step": pairs_ms, "projector_share": pairs_ms / ms,
+        "pair_gups": upd / (pairs_ms * 1e-3) / 1e9,
+        "err_last": float(np.sqrt(st[-1, :, 0].sum())), "image_rel_err_after_all_steps": rel,
+        "e2e": {"value": 1e3 / e2e_ms, "unit": "iterations/s", "h2d_bytes_per_step": 4 * (n * n + na * n) / args.steps,
+                "d2h_bytes_per_step": 4 * n * n / args.steps},
+        "gpu_launches": None, "clocks": clk.summary()}
+    if cpu is not None:
+        out["cpu_baseline"] = cpu
+    print(json.dumps(out), flush=True)
+
+
+def admm_cpu_baseline(tp, b0, n, n2):
+    """The reference's outer ADMM-TV iteration on the host, extrapolated from one
+    forward + adjoint of the compiled reference gridding C (oracle/_ref, with the
+    project's FFT stand-in: FFTW is absent) and one dense Gt(G(.)) (numpy) at full
+    size: (n2 + 1) pairs + (n2 + 2) Gt products per outer iteration."""
+    from oracle.oracle import RefLib, ref_available
+    from oracle import admm_oracle as ao
+    if not ref_available():
+        return None
+    R = RefLib()
+    deg = np.asarray(tp.angles, np.float32)
+    x = np.ones((n, n), np.float32)
+    t0 = time.perf_counter()
+    y = R.gridrec(0, x, deg, tp.param_nofilt, tp.lut, tp.deapod)
+    R.gridrec(1, y, deg, tp.param_nofilt, tp.lut, tp.deapod)
+    t_pair = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    ao.Gt(ao.G(x.astype(np.float64)))
+    t_gt = time.perf_counter() - t0
+    per_iter = (n2 + 1) * t_pair + (n2 + 2) * t_gt
+    return {"value": 1.0 / per_iter, "unit": "iterations/s", "cores": 1, "kind": "reference",
+            "sample": f"one gridding A + A^T ({t_pair:.2f} s) and one dense Gt(G) ({t_gt:.3f} s) at full size, "
+                      f"extrapolated to {n2 + 1} pairs + {n2 + 2} Gt per outer iteration; FFT: project stand-in"}
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -304,6 +408,8 @@ def main():
         return run_batch(args, rank, world, local)
     if args.workload == "warmstart":
         return run_warmstart(args, rank, world, local)
+    if args.workload == "admm":
+        return run_admm(args, rank, world, local)
 
     import torch
     import torch.distributed as dist

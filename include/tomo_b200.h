@@ -140,6 +140,37 @@ int tomo_solver_run(tomo_solver *solver, float *d_x, int iters, double *residual
                     void *stream);
 int tomo_solver_destroy(tomo_solver *solver);
 
+/* ---- ADMM / conjugate-gradient solvers (algorithms/admm.py, algorithms/cg.py) ---- */
+#define TOMO_REG_CG 1       /* cg.py:83-185: CG on A^T A x = A^T b (admm.py:245 conj_grad) */
+#define TOMO_REG_LASSO 2    /* admm.py:291-457 lasso_l1, inner cg.py:189-253 cg_lasso_l1 */
+#define TOMO_REG_LASSO_TV 3 /* admm.py:470-640 lasso_tv, inner cg.py:256-320 cg_lasso_tv */
+
+typedef struct tomo_admm_params {
+  float lambd1, lambd2, mu; /* class_admm_param.py:67-69 (float32) */
+  int n_iter_pcg;           /* inner CG iterations per ADMM iteration (-n2) */
+  float pc;                 /* -pc: < 0 off; 1: negatives to 0 and resolution circle;
+                               2: circle only; otherwise negatives times pc */
+  int i1, i2;               /* the constraint acts on x[:, i1:i2, i1:i2] */
+} tomo_admm_params;
+
+typedef struct tomo_admm tomo_admm;
+
+/* Binds an ADMM (or plain CG) solver to a plan of nz slices of one geometry
+ * and a measured sinogram d_b [nz][na][n] (device; must outlive the solver);
+ * computes A^T b once.  The arithmetic keeps the reference's numpy types
+ * (float32 x; float64 r, p for Lasso-TV; float32 scalars). */
+int tomo_admm_create(tomo_plan *plan, int reg, const float *d_b, const tomo_admm_params *prm, void *stream,
+                     tomo_admm **out);
+/* Runs `iters` ADMM iterations (Lasso-L1 / Lasso-TV: n_iter_pcg CG steps,
+ * the constraint, the shrinkage and the multiplier update) or `iters` CG
+ * iterations (TOMO_REG_CG) in place on d_x [nz][n][n].  reset != 0 starts as
+ * the reference's function does (u = alpha = 0, x_old = x; CG: r0 from x);
+ * reset == 0 continues the previous call on the same d_x.  If stats != NULL
+ * it receives [iters][nz][3]: per slice |r|^2, |x - x_old|^2, |x_old|^2 (ADMM,
+ * r the multiplier update) or |r|^2, 0, 0 (CG, r the CG residual). */
+int tomo_admm_run(tomo_admm *h, float *d_x, int iters, int reset, double *stats, int use_graph, void *stream);
+int tomo_admm_destroy(tomo_admm *h);
+
 /* Distance-driven forward projection that allocates no device memory, for
  * callers that cannot call cudaMalloc (their device memory belongs to another
  * allocator, or they must not allocate inside a latency-bound loop).  No

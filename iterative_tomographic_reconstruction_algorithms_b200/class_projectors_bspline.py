@@ -22,7 +22,7 @@ import numpy as np
 
 from . import _lib
 from .bspline_functions import init_lut_bspline
-from .filters import filter_proj
+from .filters import filter_proj, filter_proj_device
 
 myfloat = np.float32
 
@@ -89,14 +89,21 @@ class projectors:
         return self._apply(x, False)
 
     def fbp(self, x):
-        """Filtered backprojection (class_projectors_bspline.py:83-108)."""
-        x0 = np.asarray(x)[:, ::-1].copy()
+        """Filtered backprojection (class_projectors_bspline.py:83-108).
+
+        numpy input follows the reference step by step (host filtering);
+        a CUDA tensor [na, n] or [nz, na, n] is filtered on the device
+        (filters.filter_proj_device) and stays there."""
         dpc = self.radon_degree != 0
+        scale = np.pi / (1.0 * self.nang) if dpc else np.pi / (2.0 * self.nang)
+        if hasattr(x, "is_cuda") and x.is_cuda:
+            import torch
+            x0 = filter_proj_device(torch.flip(x, dims=[-1]), ftype=self.filt, dpc=dpc)
+            reco = self._apply(x0, False, which="lut0") * scale
+            return torch.flip(reco, dims=[-2, -1]).contiguous()
+        x0 = np.asarray(x)[:, ::-1].copy()
         x0[:] = filter_proj(x0, ftype=self.filt, dpc=dpc)
         reco = self._apply(x0.astype(myfloat), False, which="lut0")
-        if dpc:
-            reco = reco * (np.pi / (1.0 * self.nang))
-        else:
-            reco = reco * (np.pi / (2.0 * self.nang))
+        reco = reco * scale
         reco[:] = reco[::-1, ::-1]
         return reco

@@ -50,3 +50,17 @@ def filter_proj(sino: np.ndarray, ftype: str = "ramp", dpc: bool = False) -> np.
     out = np.real(np.fft.ifft(np.fft.fft(padded, axis=1) * filtarr[None, :], axis=1))
     sino[:, :] = out[:, :npix]
     return sino
+
+
+def filter_proj_device(sino, ftype: str = "ramp", dpc: bool = False):
+    """``filter_proj`` for a CUDA tensor [..., nang, npix]: the same float64
+    transform of the zero-padded rows (torch.fft on the device), result float32.
+    Returns a new tensor; the input is not modified."""
+    import torch
+    npix = int(sino.shape[-1])
+    nfreq = 2 * int(2 ** (int(np.ceil(np.log2(npix)))))
+    filtarr = torch.from_numpy(np.asarray(calc_filter(nfreq, ftype=ftype, dpc=dpc)).astype(np.complex128))
+    spec = torch.fft.fft(sino.to(torch.float64), n=2 * nfreq, dim=-1)
+    out = torch.fft.ifft(spec * filtarr.to(sino.device), dim=-1).real[..., :npix]
+    return out.to(torch.float32).contiguous()
+

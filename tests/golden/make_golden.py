@@ -115,5 +115,75 @@ def main() -> None:
     print("wrote", sorted(p.name for p in OUT.glob("*.npz")))
 
 
+def make_fbp() -> None:
+    """fbp_golden.npz: filtered backprojection and projection filtering.
+
+    * ``filter/<ftype>_<dpc>``: the reference's own filters.filter_proj
+      (common/operators/filters_module/filters.py:89-113, imported from the
+      reference tree) on seeded float32 projections;
+    * ``bspline/<case>``: the reference's B-spline ``fbp`` pipeline
+      (class_projectors_bspline.py:83-108): row flip, the reference's
+      filter_proj, the compiled reference backprojector with the degree-0 LUT,
+      pi/(2 na) or pi/na, 180-degree rotation;
+    * ``grid/<case>``: the compiled reference gridding adjoint with every
+      built-in filter (param[1] = 2..6) and with differential phase contrast
+      (radon_degree 1).
+    """
+    import importlib.util
+    R = RefLib()
+    rng = np.random.default_rng(20261203)
+    spec = importlib.util.spec_from_file_location(
+        "ref_filters", "/root/reference/common/operators/filters_module/filters.py")
+    if not hasattr(np, "int"):
+        np.int = int  # the reference module reads np.int at import
+    ref_filters = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(ref_filters)
+    data = {}
+    for ftype, dpc in [("ramp", False), ("shepp-logan", False), ("cosine", False), ("hamming", False),
+                       ("hanning", False), ("none", False), ("ramp", True), ("none", True)]:
+        sino = rng.standard_normal((23, 77)).astype(np.float32)
+        data[f"filter/{ftype}_{int(dpc)}/in"] = sino
+        data[f"filter/{ftype}_{int(dpc)}/out"] = ref_filters.filter_proj(sino.copy(), ftype=ftype, dpc=dpc)
+
+    for name, n, na, deg, sup, rdeg in [("n64_a90_cubic_dpc", 64, 90, 3, 4.0, 1), ("n65_a37_cubic", 65, 37, 3, 4.0, 0),
+                                        ("n48_a30_linear", 48, 30, 1, 2.0, 0)]:
+        ang = (np.arange(na) * 180.0) / np.float32(na)  # class_projectors_bspline.py:49-50
+        lut = init_lut_bspline(2048, ang, deg, rdeg, sup).astype(np.float32)
+        lut0 = init_lut_bspline(2048, ang, deg, 0, sup).astype(np.float32)
+        param = np.array([lut.shape[1], sup], np.float32)
+        sino = rng.standard_normal((na, n)).astype(np.float32)
+        x0 = sino[:, ::-1].copy()
+        x0[:] = ref_filters.filter_proj(x0, ftype="ramp", dpc=rdeg != 0)
+        reco = R.bspline(1, x0.astype(np.float32), ang.astype(np.float32), lut0, param)
+        reco = reco * (np.pi / (1.0 * na) if rdeg else np.pi / (2.0 * na))
+        data[f"bspline/{name}/cfg"] = np.array([n, na, deg, sup, rdeg], np.float64)
+        data[f"bspline/{name}/sino"] = sino
+        data[f"bspline/{name}/fbp"] = reco[::-1, ::-1].copy()
+
+    from iterative_tomographic_reconstruction_algorithms_b200 import gridrec_lut as glut
+    for name, n, na, kernel, os_, interp, W, errs, rdeg, filt in [
+            ("n72_pswf_shlo", 72, 64, "pswf", 2.0, "nn", 7.0, 1e-3, 0, 2),
+            ("n72_pswf_hann", 72, 64, "pswf", 2.0, "nn", 7.0, 1e-3, 0, 3),
+            ("n72_kb_hamm", 72, 64, "kb", 2.0, "lin", 6.0, 6e-6, 0, 4),
+            ("n90_pswf_lanc", 90, 81, "pswf", 2.0, "nn", 7.0, 1e-3, 0, 5),
+            ("n90_kb_parz", 90, 81, "kb", 1.5, "lin", 6.6, 6e-6, 0, 6),
+            ("n64_prolate_dpc_ramp", 64, 60, "prolate", 2.0, "nn", 7.0, 1e-3, 1, 1),
+            ("n64_pswf_dpc_hann", 64, 60, "pswf", 2.0, "nn", 7.0, 1e-3, 1, 3)]:
+        Wp, lut, deapod = glut.configure_regridding(n, kernel, os_, interp, W, errs)
+        param = np.array([0.0, filt, 0, os_, 0 if interp == "nn" else 1, len(lut) - 5, Wp, rdeg], np.float32)
+        deg = np.linspace(0, 180, na, endpoint=False).astype(np.float32)
+        sino = rng.standard_normal((na, n)).astype(np.float32)
+        data[f"grid/{name}/cfg"] = np.array([n, na, os_, 0 if interp == "nn" else 1, W, errs, rdeg, filt], np.float64)
+        data[f"grid/{name}/kernel"] = np.array(kernel)
+        data[f"grid/{name}/sino"] = sino
+        data[f"grid/{name}/fbp"] = R.gridrec(1, sino, deg, param, lut.astype(np.float32), deapod.astype(np.float32))
+    np.savez_compressed(OUT / "fbp_golden.npz", **data)
+    print("wrote fbp_golden.npz")
+
+
 if __name__ == "__main__":
-    main()
+    if sys.argv[1:] == ["fbp"]:
+        make_fbp()
+    else:
+        main()
+        make_fbp()
