@@ -114,11 +114,17 @@ class AdmmSolver:
                                           stream), "tomo_admm_run")
         return stats[:iters]
 
-    def __del__(self):
+    def close(self) -> None:
         h = getattr(self, "_h", None)
         if h is not None and h.value:
             _lib.lib.tomo_admm_destroy(h)
-            self._h = None
+        self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def _objective(tp, x0, b0, lambd1, lambd2, tv: bool) -> float:

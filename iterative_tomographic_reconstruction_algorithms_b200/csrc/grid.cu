@@ -59,6 +59,7 @@ struct GridState {
   float2 *filt_b = nullptr;   // adjoint filter [pdim/2]
   float2 *tw = nullptr;       // exp(-2 pi i t / pdim), t < pdim
   float2 *sorted = nullptr;   // adjoint gather: (polar angle, angle index as float bits), sorted
+  float4 *sc4 = nullptr;      // adjoint gather: per angle (sin, cos, 1/cos, 1/sin)
   float2 *H = nullptr;        // [nz][pdim][pdim]
   float2 *rows = nullptr;     // [nz][na][pdim]
   float4 *cd = nullptr;       // [nz][na][pdim/2]: Cdata1, Cdata2
@@ -302,67 +303,121 @@ __global__ void __launch_bounds__(kFftThreads) grid_fft_adj_kernel(
   }
 }
 
+// floor(x) for 0 <= x < 2^23 without the conversion pipe: x + 2^23 rounded
+// down is 2^23 + floor(x) exactly (unit spacing in [2^23, 2^24)).
+__device__ __forceinline__ float floor_small(float x, int &i) {
+  const float t = __fadd_rd(x, 8388608.0f);
+  i = __float_as_int(t) - 0x4B000000;
+  return __fsub_rn(t, 8388608.0f);
+}
+
+// lut_eval with the floor / truncation on the FMA pipe (x >= 0, same values).
+__device__ __forceinline__ float lut_eval_fast(const float *__restrict__ lut, float x, int interp) {
+  int i;
+  if (interp == 0) {
+    floor_small(__fadd_rn(x, 0.49999997f), i);
+    return __ldg(lut + i);
+  }
+  const float fl = floor_small(x, i);
+  const float w0 = __fadd_rn(__fsub_rn(1.0f, x), fl), d = __fsub_rn(x, fl);
+  return __fmaf_rn(w0, __ldg(lut + i), __fmul_rn(d, __ldg(lut + i + 1)));
+}
+
 // Adjoint step 2: every Cartesian point gathers the polar samples whose
 // window contains it (directly, or through the mirror H[pdim-iu][pdim-iv]).
-__global__ void __launch_bounds__(128) grid_gather_kernel(
-    const float4 *__restrict__ cd, float2 *__restrict__ H, const float2 *__restrict__ sc,
-    const float2 *__restrict__ sorted, const float *__restrict__ lut, int pdim, int pdim_h, int na,
-    float h, float tbl, int interp) {
-  const int IV = blockIdx.x * blockDim.x + threadIdx.x;
-  const int IU = blockIdx.y;
-  const size_t z = blockIdx.z;
-  if (IV >= pdim) return;
-  const float4 *cdz = cd + z * (size_t)na * pdim_h;
-  const float fph = (float)pdim_h;
+//
+// The reference's window of sample (U, V) is [ceil(U-h), min(floor(U+h),
+// pdim-1)] x [..V..], and the sample is skipped when ceil(U-h) < 0 or
+// ceil(V-h) < 0.  For an integer t, ceil(a) <= t <=> a <= t, t <= floor(b) <=>
+// t <= b and ceil(a) < 0 <=> a <= -1, so membership is decided by float
+// compares of the same rounded a = U - h, b = U + h.  Per angle only the w
+// with COS w and SIN w within h (+1 of margin, far above the rounding of U,
+// V and of the reciprocals) of the target's offsets are visited.
+//
+// Angles are visited in polar-angle order from the start of the target's
+// angular window (all angles when the target is within reach of the
+// centre), w ascending; a lane handles every STRIDE-th angle of that order.
+constexpr int kGatherCentre = 48;  // half-size of the central box of the adjoint gather
+
+struct GatherArgs {
+  const float4 *cd;       // [nz][na][pdim_h] direct (x, y) and mirror (z, w) values
+  float2 *H;              // [nz][pdim][pdim]
+  const float4 *sc4;      // per angle (sin, cos, 1/cos, 1/sin)
+  const float2 *sorted;   // (polar angle, angle index as float bits), ascending
+  const float *lut;
+  int pdim, pdim_h, na, interp, centre;  // centre: half-size of the box done by warps
+  float h, tbl;
+};
+
+template <int STRIDE>
+__device__ __forceinline__ void gather_point(const GatherArgs &A, int IU, int IV, size_t z, int lane, float &hr,
+                                             float &hi) {
+  const float4 *cdz = A.cd + z * (size_t)A.na * A.pdim_h;
+  const int pdim = A.pdim, pdim_h = A.pdim_h, na = A.na;
+  const float h = A.h, fph = (float)pdim_h;
   const float reach = h * 1.41421356f + 1.0f;
-  float hr = 0.0f, hi = 0.0f;
   for (int mirror = 0; mirror < 2; ++mirror) {
     // the window point the sample must contain, and its offset from the centre
     const int tu = mirror ? pdim - IU : IU, tv = mirror ? pdim - IV : IV;
     if (mirror && (IU == 0 || IV == 0)) continue;  // targets pdim - 0 are outside the grid
+    const float ftu = (float)tu, ftv = (float)tv;
     const float du = (float)(tu - pdim_h), dv = (float)(tv - pdim_h);
     const float rho = sqrtf(du * du + dv * dv);
-    int a0 = 0, cnt = na;
-    float phi = 0.0f;
-    if (rho > reach + 1.0f) {
+    const bool windowed = rho > reach + 1.0f;
+    int a0 = 0;
+    float phi = 0.0f, dmax = 0.0f;
+    if (windowed) {
       phi = atan2f(dv, du);
       if (phi < 0.0f) phi += 6.2831853f;
-      const float delta = asinf(fminf(1.0f, reach / rho)) + 1e-3f;
-      // first sorted angle >= phi - delta (with wrap-around)
-      float lo = phi - delta;
+      dmax = asinf(fminf(1.0f, reach / rho)) + 1e-3f;
+      // first sorted angle >= phi - dmax (with wrap-around)
+      float lo = phi - dmax;
       if (lo < 0.0f) lo += 6.2831853f;
       int l = 0, r = na;
       while (l < r) {
         const int m = (l + r) >> 1;
-        if (sorted[m].x < lo) l = m + 1;
+        if (A.sorted[m].x < lo) l = m + 1;
         else r = m;
       }
       a0 = l;
-      cnt = na;  // bounded below by the angular test
     }
-    for (int t = 0; t < cnt; ++t) {
+    const float wbase = mirror ? 1.0f : 0.0f;
+    // the in-window angles are a prefix of the cyclic order from a0
+    for (int t = lane; t < na; t += STRIDE) {
       int si = a0 + t;
       if (si >= na) si -= na;
-      const float2 e = sorted[si];
-      if (rho > reach + 1.0f) {
+      const float2 e = A.sorted[si];
+      if (windowed) {
         float dphi = fabsf(e.x - phi);
         dphi = fminf(dphi, 6.2831853f - dphi);
-        if (dphi > asinf(fminf(1.0f, reach / rho)) + 1e-3f) break;  // left the window
+        if (dphi > dmax) break;  // left the window
       }
       const int n = __float_as_int(e.y);
-      const float2 ang = sc[n];
+      const float4 ang = A.sc4[n];  // SIN, COS, 1/COS, 1/SIN
       const float SIN = ang.x, COS = ang.y;
       const float tt = du * COS + dv * SIN;  // along-ray position of the target
-      int w0 = max((int)floorf(tt - reach), mirror ? 1 : 0), w1 = min((int)ceilf(tt + reach), pdim_h - 1);
-      for (int w = w0; w <= w1; ++w) {
-        const float U = __fmaf_rn(COS, (float)w, fph), V = __fmaf_rn(SIN, (float)w, fph);
-        const float cu = ceilf(__fsub_rn(U, h)), cv = ceilf(__fsub_rn(V, h));
-        if (cu < 0.0f || cv < 0.0f) continue;  // the reference skips this sample entirely
-        const int iuh = min((int)floorf(__fadd_rn(h, U)), pdim - 1);
-        const int ivh = min((int)floorf(__fadd_rn(V, h)), pdim - 1);
-        if (tu < (int)cu || tu > iuh || tv < (int)cv || tv > ivh) continue;
-        const float rt = lut_eval(lut, __fmul_rn(fabsf(__fsub_rn(U, (float)tu)), tbl), interp);
-        const float wk = lut_eval(lut, __fmul_rn(fabsf(__fsub_rn(V, (float)tv)), tbl), interp);
+      float lo = tt - reach, hi2 = tt + reach;
+      if (fabsf(COS) >= 1e-2f) {
+        const float a = (du - h) * ang.z, b = (du + h) * ang.z;
+        lo = fmaxf(lo, fminf(a, b) - 1.0f);
+        hi2 = fminf(hi2, fmaxf(a, b) + 1.0f);
+      }
+      if (fabsf(SIN) >= 1e-2f) {
+        const float a = (dv - h) * ang.w, b = (dv + h) * ang.w;
+        lo = fmaxf(lo, fminf(a, b) - 1.0f);
+        hi2 = fminf(hi2, fmaxf(a, b) + 1.0f);
+      }
+      lo = fmaxf(ceilf(lo), wbase);
+      hi2 = fminf(floorf(hi2), (float)(pdim_h - 1));
+      if (lo > hi2) continue;
+      int w = (int)lo;
+      for (float wf = lo; wf <= hi2; wf += 1.0f, ++w) {
+        const float U = __fmaf_rn(COS, wf, fph), V = __fmaf_rn(SIN, wf, fph);
+        const float ua = __fsub_rn(U, h), va = __fsub_rn(V, h);
+        if (ua <= -1.0f || va <= -1.0f) continue;  // the reference skips this sample entirely
+        if (ua > ftu || __fadd_rn(h, U) < ftu || va > ftv || __fadd_rn(V, h) < ftv) continue;
+        const float rt = lut_eval_fast(A.lut, __fmul_rn(fabsf(__fsub_rn(U, ftu)), A.tbl), A.interp);
+        const float wk = lut_eval_fast(A.lut, __fmul_rn(fabsf(__fsub_rn(V, ftv)), A.tbl), A.interp);
         const float conv = __fmul_rn(rt, wk);
         const float4 c = cdz[(size_t)n * pdim_h + w];
         if (!mirror) {
@@ -375,7 +430,36 @@ __global__ void __launch_bounds__(128) grid_gather_kernel(
       }
     }
   }
-  H[z * (size_t)pdim * pdim + (size_t)IU * pdim + IV] = make_float2(hr, hi);
+}
+
+// One thread per Cartesian point outside the central box.
+__global__ void __launch_bounds__(128) grid_gather_kernel(GatherArgs A) {
+  const int IV = blockIdx.x * blockDim.x + threadIdx.x;
+  const int IU = blockIdx.y;
+  const size_t z = blockIdx.z;
+  if (IV >= A.pdim) return;
+  if (abs(IU - A.pdim_h) <= A.centre && abs(IV - A.pdim_h) <= A.centre) return;  // grid_gather_centre_kernel
+  float hr = 0.0f, hi = 0.0f;
+  gather_point<1>(A, IU, IV, z, 0, hr, hi);
+  A.H[z * (size_t)A.pdim * A.pdim + (size_t)IU * A.pdim + IV] = make_float2(hr, hi);
+}
+
+// One warp per point of the central box, where every angle's first samples
+// overlap and a point gathers thousands of them: lanes take every 32nd angle
+// and the partial sums are combined by a fixed butterfly (deterministic).
+__global__ void __launch_bounds__(128) grid_gather_centre_kernel(GatherArgs A) {
+  const int side = 2 * A.centre + 1;
+  const int p = blockIdx.x * 4 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+  const size_t z = blockIdx.y;
+  if (p >= side * side) return;  // warp-uniform
+  const int IU = A.pdim_h - A.centre + p / side, IV = A.pdim_h - A.centre + p % side;
+  float hr = 0.0f, hi = 0.0f;
+  gather_point<32>(A, IU, IV, z, lane, hr, hi);
+  for (int off = 16; off; off >>= 1) {
+    hr = __fadd_rn(hr, __shfl_xor_sync(0xffffffffu, hr, off));
+    hi = __fadd_rn(hi, __shfl_xor_sync(0xffffffffu, hi, off));
+  }
+  if (lane == 0) A.H[z * (size_t)A.pdim * A.pdim + (size_t)IU * A.pdim + IV] = make_float2(hr, hi);
 }
 
 // Adjoint step 4: deapodise, crop and flip (gridrec_v4_backproj.c:440-491).
@@ -520,6 +604,7 @@ static void grid_free(void *ext) {
   cudaFree(g->filt_b);
   cudaFree(g->tw);
   cudaFree(g->sorted);
+  cudaFree(g->sc4);
   cudaFree(g->H);
   cudaFree(g->rows);
   cudaFree(g->cd);
@@ -570,11 +655,13 @@ int grid_setup(Plan &p) {
   for (int i = 0; i < g->nfac; ++i) g->fac[i] = f[i];
   // per-angle sin/cos (double sincos of deg * pi/180, as compiled)
   std::vector<float2> sc(na);
+  std::vector<float4> sc4(na);
   std::vector<std::pair<float, int>> order(na);
   for (int n = 0; n < na; ++n) {
     const double t = (double)p.angles[n] * 0.017453292519943295;
     const float s = (float)std::sin(t), c = (float)std::cos(t);
     sc[n] = make_float2(s, c);
+    sc4[n] = make_float4(s, c, c != 0.0f ? 1.0f / c : 0.0f, s != 0.0f ? 1.0f / s : 0.0f);
     float phi = std::atan2(s, c);
     if (phi < 0) phi += 6.2831853f;
     order[n] = {phi, n};
@@ -620,6 +707,7 @@ int grid_setup(Plan &p) {
   if ((rc = up((void **)&g->deapod, G.grid_deapod, sizeof(float) * (size_t)pdim * pdim))) return rc;
   if ((rc = up((void **)&g->sc, sc.data(), sizeof(float2) * na))) return rc;
   if ((rc = up((void **)&g->sorted, sorted.data(), sizeof(float2) * na))) return rc;
+  if ((rc = up((void **)&g->sc4, sc4.data(), sizeof(float4) * na))) return rc;
   if ((rc = up((void **)&g->filt_f, ff.data(), sizeof(float2) * ff.size()))) return rc;
   if ((rc = up((void **)&g->filt_b, fb.data(), sizeof(float2) * fb.size()))) return rc;
   if ((rc = up((void **)&g->tw, tw.data(), sizeof(float2) * tw.size()))) return rc;
@@ -671,9 +759,12 @@ int grid_adjoint(Plan &p, const float *d_sino, float *d_img, cudaStream_t s, con
   grid_fft_adj_kernel<<<na * nz, kFftThreads, smem, s>>>(d_sino, g.cd, g.tw, g.filt_b, fft_const(g), npix,
                                                          g.padleft, g.pdim_h, g.radon_degree,
                                                          (float)(1.0 / pdim));
+  GatherArgs ga{g.cd, g.H, g.sc4, g.sorted, g.lut, pdim, g.pdim_h, na, g.interp, 0, g.h_b, g.tbl_b};
+  ga.centre = std::min(kGatherCentre, g.pdim_h - 1);
+  const int side = 2 * ga.centre + 1;
+  grid_gather_centre_kernel<<<dim3((side * side + 3) / 4, nz), 128, 0, s>>>(ga);
   dim3 gb(128), gg((pdim + 127) / 128, pdim, nz);
-  grid_gather_kernel<<<gg, gb, 0, s>>>(g.cd, g.H, g.sc, g.sorted, g.lut, pdim, g.pdim_h, na, g.h_b, g.tbl_b,
-                                       g.interp);
+  grid_gather_kernel<<<gg, gb, 0, s>>>(ga);
   if (cufftSetStream(g.fft2, s) != CUFFT_SUCCESS ||
       cufftExecC2C(g.fft2, (cufftComplex *)g.H, (cufftComplex *)g.H, CUFFT_INVERSE) != CUFFT_SUCCESS)
     return fail(TOMO_ECUDA, "grid: 2-D FFT failed");
