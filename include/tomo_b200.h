@@ -109,6 +109,12 @@ int tomo_plan_layout(tomo_plan *plan, int *instances, size_t *img_off, size_t *s
  * kernels, chosen at plan creation by timing the candidates on the plan's own
  * scratch when the workload is large enough), as text. */
 int tomo_plan_tuning(tomo_plan *plan, char *buf, size_t len);
+/* Pins the launch shape of a distance-driven plan by name instead of the
+ * tuned one (NULL keeps a direction as it is): forward "w2w" "w4w" "w8w"
+ * "w2b" "w4b" "w8b" (warps per block, warp or block fetch of work items);
+ * adjoint "t1" "t2" "t4" (pixel tiles per block, 4 warps per tile).  Every
+ * shape gives the same result to the bit; other kinds: TOMO_EINVAL. */
+int tomo_plan_set_tuning(tomo_plan *plan, const char *fwd, const char *adj);
 
 /* Forward A: d_image [nz][n][n] -> d_sino [nz][na][n] (overwritten). */
 int tomo_forward(tomo_plan *plan, const float *d_image, float *d_sino, void *stream);

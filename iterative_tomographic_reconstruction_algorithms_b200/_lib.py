@@ -82,6 +82,7 @@ def _load() -> ctypes.CDLL:
     lib.tomo_plan_layout.argtypes = [vp, ctypes.POINTER(i), ctypes.POINTER(ctypes.c_size_t),
                                      ctypes.POINTER(ctypes.c_size_t), ctypes.c_size_t]
     lib.tomo_plan_tuning.argtypes = [vp, ctypes.c_char_p, ctypes.c_size_t]
+    lib.tomo_plan_set_tuning.argtypes = [vp, ctypes.c_char_p, ctypes.c_char_p]
     return lib
 
 
@@ -186,6 +187,14 @@ class Plan:
     def adjoint(self, y):
         return self._run(y, False)
 
+    def tuning(self) -> str:
+        return plan_tuning(self)
+
+    def set_tuning(self, fwd: str | None = None, adj: str | None = None) -> None:
+        """Pins the distance-driven launch shapes by name (``tomo_plan_set_tuning``)."""
+        check(lib.tomo_plan_set_tuning(self._h, fwd.encode() if fwd else None, adj.encode() if adj else None),
+              "tomo_plan_set_tuning")
+
 
 class BatchPlan(Plan):
     """Distance-driven plan over geometries of different sizes (``tomo_plan_create_batch``).
@@ -249,9 +258,6 @@ class BatchPlan(Plan):
     @property
     def sino_shape(self):
         return (self.sino_total,)
-
-    def tuning(self) -> str:
-        return plan_tuning(self)
 
 
 def plan_tuning(plan: Plan) -> str:

@@ -148,7 +148,7 @@ __global__ void __launch_bounds__(128) dd_forward_kernel(
 // Instances
 // ---------------------------------------------------------------------------
 constexpr int kGrpDet = 127;              // detectors per forward item (128 boundaries, 4 per lane)
-constexpr int kTileW = 16, kTileH = 8;    // pixels per adjoint item (2x2 per lane, 8x4 lanes)
+constexpr int kTileW = 32, kTileH = 16;   // pixels per adjoint item (4x4 per lane, 8x4 lanes)
 constexpr int kScanThreads = 256;
 constexpr int kColWarps = 4, kColRows = 16;
 // Adding 1.5 * 2^23 rounds a float of magnitude < 2^22 to an integer held in
@@ -499,35 +499,38 @@ __global__ void __launch_bounds__(32 * W) dd_fwd_kernel(const DdInst *__restrict
 }
 
 // ---------------------------------------------------------------------------
-// Adjoint: a warp item is a 16x8 pixel tile; lane l holds the 2x2 pixels at
-// rows a0, a0+1 and columns b0, b0+1.  Per angle and line each pixel [P0, P1]
+// Adjoint: a warp item is a 32x16 pixel tile; lane l holds the 4x4 pixels at
+// rows a0..a0+3 and columns b0..b0+3.  Per angle and line each pixel [P0, P1]
 // overlaps the detector a holding P0 and possibly a+1 (detectors are at least
 // one pixel wide): (min(D_a+1, P1) - P0) S_a + (P1 - min(D_a+1, P1)) S_a+1,
-// the reference's two gaps.
+// the reference's two gaps, both accumulated by FMA.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ float dd_adj_pixel(float P0, float P1, float z, float r, float cm,
-                                              const float2 *__restrict__ rowm) {
-  // a = floor(P0 z + nh) by rounding at 1.5 * 2^23 (f = kMagic + a), read as
-  // the float's bits (rowm is the row base minus kMagicBits entries); one off
-  // at a detector boundary only moves a zero-width piece
-  const float f = __fadd_rn(__fmaf_rn(P0, z, -0.5f), cm);
+__device__ __forceinline__ void dd_adj_pixel(float P0, float P1, float z, float r, float cm, float cm1,
+                                             const float2 *__restrict__ rowm, float &acc) {
+  // f = cm + floor(P0 z) exactly: rounded down in [2^23, 2^24), where floats
+  // are the integers; a = floor(P0 z + nh) is f's bits minus kMagicBits (rowm
+  // is the row base minus kMagicBits entries)
+  const float f = __fmaf_rd(P0, z, cm);
   const float2 t = __ldg(rowm + __float_as_int(f));  // {S_a, S_a+1}
   // D_a+1 = (a + 1 - nh) r, with a + 1 - nh = f - (kMagic + nh - 1) exactly
-  const float D1 = __fmul_rn(__fsub_rn(f, __fsub_rn(cm, 1.0f)), r);
+  const float D1 = __fmul_rn(__fsub_rn(f, cm1), r);
   const float m = fminf(D1, P1);
-  return fmaf(__fsub_rn(P1, m), t.y, __fmul_rn(__fsub_rn(m, P0), t.x));
+  acc = __fmaf_rn(__fsub_rn(m, P0), t.x, acc);
+  acc = __fmaf_rn(__fsub_rn(P1, m), t.y, acc);
 }
 
 template <bool COLS>
 __device__ __forceinline__ void dd_adj_pass(const float4 *__restrict__ tab, int cnt,
                                             const float2 *__restrict__ AS, int a0, int b0, int n, int nh,
-                                            float (&acc)[2][2]) {
+                                            float (&acc)[4][4]) {
   const int l0 = COLS ? b0 : a0, k0 = COLS ? a0 : b0;
-  const float y0 = (float)(l0 - nh) + 0.5f, y1 = __fadd_rn(y0, 1.0f);
-  const float x0 = (float)(k0 - nh), x1 = __fadd_rn(x0, 1.0f), x2 = __fadd_rn(x0, 2.0f);
-  const bool lastpix = k0 + 1 >= n - 1;
-  const float cm = kMagic + (float)nh;
-#pragma unroll 2
+  const float y0 = (float)(l0 - nh) + 0.5f;
+  float x[5];
+#pragma unroll
+  for (int j = 0; j < 5; ++j) x[j] = (float)(k0 - nh + j);
+  const bool lastpix = k0 + 3 >= n - 1;
+  const float cm = kMagic + (float)nh, cm1 = cm - 1.0f;
+#pragma unroll 1
   for (int u = 0; u < cnt; ++u) {
     const float4 e = __ldg(tab + u);
     const float r = e.x, k = e.y, z = e.z;
@@ -535,76 +538,109 @@ __device__ __forceinline__ void dd_adj_pass(const float4 *__restrict__ tab, int 
     const float2 *rowm = row - kMagicBits;
     const float Dn = det_bound(n, nh, r);
 #pragma unroll
-    for (int li = 0; li < 2; ++li) {
-      const float q = __fmul_rn(li ? y1 : y0, k);
-      const float P0 = __fsub_rn(x0, q), P1 = __fsub_rn(x1, q), P2 = __fsub_rn(x2, q);
-      float s0 = dd_adj_pixel(P0, P1, z, r, cm, rowm), s1 = dd_adj_pixel(P1, P2, z, r, cm, rowm);
-      if (lastpix || (P0 < Dn && Dn < P2)) {
+    for (int li = 0; li < 4; ++li) {
+      const float q = __fmul_rn(__fadd_rn(y0, (float)li), k);
+      float P[5];
+#pragma unroll
+      for (int j = 0; j < 5; ++j) P[j] = __fsub_rn(x[j], q);
+#pragma unroll
+      for (int j = 0; j < 4; ++j) dd_adj_pixel(P[j], P[j + 1], z, r, cm, cm1, rowm, COLS ? acc[j][li] : acc[li][j]);
+      if (lastpix || (P[0] < Dn && Dn < P[4])) {
         DdDrop d;
         if (dd_dropped_piece(q, r, n, nh, d)) {
           const float sd = __fmul_rn(d.gap, __ldg(&row[d.det].x));
-          if (d.pix == k0) s0 -= sd;
-          else if (d.pix == k0 + 1) s1 -= sd;
+#pragma unroll
+          for (int j = 0; j < 4; ++j)  // unrolled: acc stays in registers
+            if (d.pix == k0 + j) (COLS ? acc[j][li] : acc[li][j]) -= sd;
         }
       }
-      if (COLS) {
-        acc[0][li] += s0;
-        acc[1][li] += s1;
-      } else {
-        acc[li][0] += s0;
-        acc[li][1] += s1;
+    }
+  }
+}
+
+// One item = one 32x16 tile, worked on by 4 warps: warp `quarter` sums the
+// angles [quarter T / 4, (quarter + 1) T / 4) of the ROWS-then-COLS order (T =
+// nR + nC), and the tile's first warp adds the quarters in order, then the
+// row / column sums, then stores.  The split never depends on the launch
+// shape, so every shape gives the same bits.
+template <int TB>
+__global__ void __launch_bounds__(128 * TB) dd_adj_kernel(const DdInst *__restrict__ inst, int ninst,
+                                                           long long nitems, unsigned long long *__restrict__ ctr,
+                                                           const double2 *__restrict__ work,
+                                                           float *__restrict__ img, AdjEpi ep) {
+  __shared__ long long base_s;
+  __shared__ float part[TB][3][16][32];  // quarters 1..3 of each tile
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int tile = warp >> 2, quarter = warp & 3;
+  for (;;) {
+    if (threadIdx.x == 0) base_s = (long long)atomicAdd(ctr, (unsigned long long)TB);
+    __syncthreads();
+    const long long first = base_s;
+    __syncthreads();
+    if (first >= nitems) break;  // block-uniform
+    const long long item = first + tile;
+    float acc[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) acc[i][j] = 0.0f;
+    const DdInst *Ip = nullptr;
+    int a0 = 0, b0 = 0;
+    bool inside = false;
+    if (item < nitems) {
+      Ip = &inst[find_inst(inst, ninst, item, &DdInst::a0)];
+      const DdInst &I = *Ip;
+      const int local = (int)(item - I.a0);
+      b0 = (local % I.tx) * kTileW + 4 * (lane & 7);
+      a0 = (local / I.tx) * kTileH + 4 * (lane >> 3);
+      // lanes whose block starts outside the image (n not a multiple of 4)
+      // only take part in the epilogue's warp reductions
+      inside = a0 < I.n && b0 < I.n;
+      if (inside) {
+        const int T = I.nR + I.nC;
+        const int u0 = (int)((long long)T * quarter / 4), u1 = (int)((long long)T * (quarter + 1) / 4);
+        const float2 *AS = (const float2 *)(work + I.as) + I.pads;
+        const int r0 = min(u0, I.nR), r1 = min(u1, I.nR);
+        if (r1 > r0) dd_adj_pass<false>(I.tab + r0, r1 - r0, AS, a0, b0, I.n, I.nh, acc);
+        const int c0 = max(u0, I.nR), c1 = max(u1, I.nR);
+        if (c1 > c0) dd_adj_pass<true>(I.tab + c0, c1 - c0, AS, a0, b0, I.n, I.nh, acc);
       }
     }
-  }
-}
-
-__device__ __forceinline__ void dd_adj_item(const DdInst &I, int txi, int tyi, int lane,
-                                            const double2 *__restrict__ work, float *__restrict__ img,
-                                            const AdjEpi &ep) {
-  const int n = I.n, nh = I.nh;
-  const int b0 = txi * kTileW + 2 * (lane & 7), a0 = tyi * kTileH + 2 * (lane >> 3);
-  float acc[2][2] = {{0.0f, 0.0f}, {0.0f, 0.0f}};
-  const float2 *AS = (const float2 *)(work + I.as) + I.pads;
-  // tiles that start outside the image (n not a multiple of the tile) only
-  // take part in the epilogue's warp reductions
-  const bool inside = a0 < n && b0 < n;
-  if (inside) {
-    dd_adj_pass<false>(I.tab, I.nR, AS, a0, b0, n, nh, acc);
-    dd_adj_pass<true>(I.tab + I.nR, I.nC, AS, a0, b0, n, nh, acc);
-  }
-  for (int t = 0; inside && t < I.nS; ++t) {  // row / column sums (|sin| or |cos| < 1e-7)
-    const int2 e = __ldg(I.tabS + t);
-    const float2 *row = AS + e.y;
+    if (quarter > 0) {
 #pragma unroll
-    for (int i = 0; i < 2; ++i)
+      for (int i = 0; i < 4; ++i)
 #pragma unroll
-      for (int j = 0; j < 2; ++j) acc[i][j] += __ldg(&row[e.x == DD_ROWSUM ? a0 + i : b0 + j].x);
-  }
-#pragma unroll
-  for (int i = 0; i < 2; ++i)
-#pragma unroll
-    for (int j = 0; j < 2; ++j) {
-      const int a = a0 + i, b = b0 + j;
-      const bool live = a < n && b < n;
-      adj_store(ep, acc[i][j], live, (size_t)I.img + (size_t)(live ? a : 0) * n + (live ? b : 0), img);
+        for (int j = 0; j < 4; ++j) part[tile][quarter - 1][4 * i + j][lane] = acc[i][j];
     }
-}
-
-template <int W, bool BLOCK>
-__global__ void __launch_bounds__(32 * W) dd_adj_kernel(const DdInst *__restrict__ inst, int ninst,
-                                                         long long nitems, unsigned long long *__restrict__ ctr,
-                                                         const double2 *__restrict__ work,
-                                                         float *__restrict__ img, AdjEpi ep) {
-  __shared__ long long base_s;
-  const int lane = threadIdx.x & 31;
-  for (;;) {
-    const long long item = fetch_item<BLOCK>(ctr, W, &base_s);
-    if (item - (BLOCK ? (threadIdx.x >> 5) : 0) >= nitems) break;
-    if (item < nitems) {
-      const DdInst &I = inst[find_inst(inst, ninst, item, &DdInst::a0)];
-      const int local = (int)(item - I.a0);
-      dd_adj_item(I, local % I.tx, local / I.tx, lane, work, img, ep);
+    __syncthreads();
+    if (quarter == 0 && Ip) {
+      const DdInst &I = *Ip;
+      const int n = I.n;
+#pragma unroll
+      for (int q = 0; q < 3; ++q)
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+          for (int j = 0; j < 4; ++j) acc[i][j] += part[tile][q][4 * i + j][lane];
+      const float2 *AS = (const float2 *)(work + I.as) + I.pads;
+      for (int t = 0; inside && t < I.nS; ++t) {  // row / column sums (|sin| or |cos| < 1e-7)
+        const int2 e = __ldg(I.tabS + t);
+        const float2 *row = AS + e.y;
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+          for (int j = 0; j < 4; ++j) acc[i][j] += __ldg(&row[e.x == DD_ROWSUM ? a0 + i : b0 + j].x);
+      }
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const int a = a0 + i, b = b0 + j;
+          const bool live = inside && a < n && b < n;
+          adj_store(ep, acc[i][j], live, (size_t)I.img + (size_t)(live ? a : 0) * n + (live ? b : 0), img);
+        }
     }
+    __syncthreads();  // part[] is rewritten by the next item
   }
 }
 
@@ -684,32 +720,38 @@ using FwdFn = void (*)(const DdInst *, int, long long, unsigned long long *, con
                       FwdEpi);
 using AdjFn = void (*)(const DdInst *, int, long long, unsigned long long *, const double2 *, float *,
                       AdjEpi);
+// Launch shapes the autotuner chooses from.  Forward: warps per block x
+// fetch mode.  Adjoint: tiles per block (4 warps each).
 struct DdCfg {
   int W;
   bool block;
   FwdFn fwd;
-  AdjFn adj;
 };
-// Launch shapes the autotuner chooses from: warps per block x fetch mode.
 const DdCfg kDdCfg[] = {
-    {2, false, dd_fwd_kernel<2, false>, dd_adj_kernel<2, false>},
-    {4, false, dd_fwd_kernel<4, false>, dd_adj_kernel<4, false>},
-    {8, false, dd_fwd_kernel<8, false>, dd_adj_kernel<8, false>},
-    {2, true, dd_fwd_kernel<2, true>, dd_adj_kernel<2, true>},
-    {4, true, dd_fwd_kernel<4, true>, dd_adj_kernel<4, true>},
-    {8, true, dd_fwd_kernel<8, true>, dd_adj_kernel<8, true>},
+    {2, false, dd_fwd_kernel<2, false>}, {4, false, dd_fwd_kernel<4, false>}, {8, false, dd_fwd_kernel<8, false>},
+    {2, true, dd_fwd_kernel<2, true>},   {4, true, dd_fwd_kernel<4, true>},   {8, true, dd_fwd_kernel<8, true>},
 };
 constexpr int kNumCfg = (int)(sizeof(kDdCfg) / sizeof(kDdCfg[0]));
-
-std::string cfg_name(int c) { return "w" + std::to_string(kDdCfg[c].W) + (kDdCfg[c].block ? "b" : "w"); }
+struct AdjCfg {
+  int TB;
+  AdjFn adj;
+};
+const AdjCfg kAdjCfg[] = {{1, dd_adj_kernel<1>}, {2, dd_adj_kernel<2>}, {4, dd_adj_kernel<4>}};
+constexpr int kNumAdj = (int)(sizeof(kAdjCfg) / sizeof(kAdjCfg[0]));
+int num_cfg(bool fwd) { return fwd ? kNumCfg : kNumAdj; }
+std::string cfg_name(int c, bool fwd = true) {
+  if (!fwd) return "t" + std::to_string(kAdjCfg[c].TB);
+  return "w" + std::to_string(kDdCfg[c].W) + (kDdCfg[c].block ? "b" : "w");
+}
+int cfg_threads(int c, bool fwd) { return fwd ? 32 * kDdCfg[c].W : 128 * kAdjCfg[c].TB; }
 
 // Persistent grid: as many blocks as fit on the device at once.
 int dd_grid(int c, bool fwd, int *grid) {
   int dev = 0, sms = 0, nb = 0;
   TOMO_CUDA(cudaGetDevice(&dev));
   TOMO_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-  const void *k = fwd ? (const void *)kDdCfg[c].fwd : (const void *)kDdCfg[c].adj;
-  TOMO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, 32 * kDdCfg[c].W, 0));
+  const void *k = fwd ? (const void *)kDdCfg[c].fwd : (const void *)kAdjCfg[c].adj;
+  TOMO_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, cfg_threads(c, fwd), 0));
   *grid = std::max(1, nb) * sms;
   return TOMO_OK;
 }
@@ -726,8 +768,8 @@ int dd_launch_fwd(const DdState &S, int c, int grid, const double2 *work, float 
 int dd_launch_adj(const DdState &S, int c, int grid, const double2 *work, float *img, cudaStream_t s,
                   const AdjEpi &ep) {
   TOMO_CUDA(cudaMemsetAsync(S.d_ctr + 1, 0, sizeof(unsigned long long), s));
-  kDdCfg[c].adj<<<grid, 32 * kDdCfg[c].W, 0, s>>>(S.d_inst, (int)S.inst.size(), S.adj_items, S.d_ctr + 1,
-                                                    work, img, ep);
+  kAdjCfg[c].adj<<<grid, cfg_threads(c, false), 0, s>>>(S.d_inst, (int)S.inst.size(), S.adj_items,
+                                                         S.d_ctr + 1, work, img, ep);
   TOMO_CUDA(cudaGetLastError());
   return TOMO_OK;
 }
@@ -772,7 +814,7 @@ int dd_autotune(Plan &p, DdState &S) {
     for (int dir = 0; dir < 2 && rc == TOMO_OK; ++dir) {
       float best = 1e30f;
       log += dir == 0 ? "fwd" : "; adj";
-      for (int c = 0; c < kNumCfg && rc == TOMO_OK; ++c) {
+      for (int c = 0; c < num_cfg(dir == 0) && rc == TOMO_OK; ++c) {
         int grid = 0;
         if ((rc = dd_grid(c, dir == 0, &grid))) break;
         float ms = 0.0f;
@@ -787,7 +829,7 @@ int dd_autotune(Plan &p, DdState &S) {
           if (rep) ms += t;
         }
         char buf[48];
-        std::snprintf(buf, sizeof(buf), " %s=%.3fms", cfg_name(c).c_str(), ms / 2);
+        std::snprintf(buf, sizeof(buf), " %s=%.3fms", cfg_name(c, dir == 0).c_str(), ms / 2);
         log += buf;
         if (ms < best) {
           best = ms;
@@ -808,7 +850,8 @@ int dd_autotune(Plan &p, DdState &S) {
   if (S.tuning.empty()) S.tuning = "default (small workload)";
   int rc = dd_grid(S.wf, true, &S.grid_f);
   if (!rc) rc = dd_grid(S.wa, false, &S.grid_a);
-  S.tuning = "fwd " + cfg_name(S.wf) + ", adj " + cfg_name(S.wa) + " (w<warps/block> + b: block fetch, w: warp fetch)" +
+  S.tuning = "fwd " + cfg_name(S.wf) + ", adj " + cfg_name(S.wa, false) +
+             " (forward w<warps/block> + b: block fetch, w: warp fetch; adjoint t<tiles/block>)" +
              ", grids " + std::to_string(S.grid_f) + "/" + std::to_string(S.grid_a) + " (" + S.tuning + ")";
   return rc;
 }
@@ -981,6 +1024,28 @@ int dd_layout(const Plan &p, int *instances, size_t *img_off, size_t *sino_off, 
 }
 
 const std::string &dd_tuning(const Plan &p) { return ((const DdState *)p.ext)->tuning; }
+
+int dd_set_tuning(Plan &p, const char *fwd, const char *adj) {
+  DdState &S = *(DdState *)p.ext;
+  int wf = S.wf, wa = S.wa;
+  for (int dir = 0; dir < 2; ++dir) {
+    const char *name = dir == 0 ? fwd : adj;
+    if (!name) continue;
+    int found = -1;
+    for (int c = 0; c < num_cfg(dir == 0); ++c)
+      if (cfg_name(c, dir == 0) == name) found = c;
+    if (found < 0) return fail(TOMO_EINVAL, std::string("set_tuning: unknown ") + (dir ? "adjoint" : "forward") +
+                                                " shape '" + name + "'");
+    (dir == 0 ? wf : wa) = found;
+  }
+  int rc = dd_grid(wf, true, &S.grid_f);
+  if (!rc) rc = dd_grid(wa, false, &S.grid_a);
+  if (rc) return rc;
+  S.wf = wf;
+  S.wa = wa;
+  S.tuning = "fwd " + cfg_name(wf) + ", adj " + cfg_name(wa, false) + " (set by the caller)";
+  return TOMO_OK;
+}
 
 int dd_forward(Plan &p, const float *d_img, float *d_sino, cudaStream_t s, const FwdEpi &ep) {
   const DdState &S = *(const DdState *)p.ext;

@@ -212,6 +212,12 @@ int tomo_plan_tuning(tomo_plan *plan, char *buf, size_t len) {
   return TOMO_OK;
 }
 
+int tomo_plan_set_tuning(tomo_plan *plan, const char *fwd, const char *adj) {
+  if (!plan) return fail(TOMO_EINVAL, "set_tuning: NULL plan");
+  if (plan->p.g.kind != TOMO_KIND_DD) return fail(TOMO_EINVAL, "set_tuning: only distance-driven plans have shapes");
+  return dd_set_tuning(plan->p, fwd, adj);
+}
+
 int tomo_plan_destroy(tomo_plan *plan) {
   if (!plan) return TOMO_OK;
   release(plan->p);

@@ -123,6 +123,7 @@ TOMO_DECLARE_KIND(grid)  // grid.cu
 int dd_setup_batch(Plan &p, const tomo_geom *geoms, int count);
 int dd_layout(const Plan &p, int *instances, size_t *img_off, size_t *sino_off, size_t cap);
 const std::string &dd_tuning(const Plan &p);
+int dd_set_tuning(Plan &p, const char *fwd, const char *adj);
 
 // Plan-less pieces of the dd forward (radon_dd.cu), used by dd_noalloc.cu.
 int dd_build_table(const float *angles, int na, DdAngle *tab);

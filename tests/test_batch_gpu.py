@@ -96,3 +96,53 @@ def test_batched_sirt_equals_single_sirt(cuda):
             assert torch.equal(xs[i], x1[0]), (n, na, z)
             i += 1
     assert res[-1] < res[0]
+
+
+FWD_SHAPES = ["w2w", "w4w", "w8w", "w2b", "w4b", "w8b"]
+ADJ_SHAPES = ["t1", "t2", "t4"]
+
+
+def test_every_launch_shape_gives_the_same_bits(cuda):
+    """Every forward / adjoint launch shape the autotuner may pick, on single
+    plans (odd and even sides, special angles, several slices) and on the
+    uneven batch."""
+    torch = cuda
+    from iterative_tomographic_reconstruction_algorithms_b200 import _lib
+    rng = np.random.default_rng(11)
+    special = np.array([0.0, 30.0, 45.0, 60.0, 90.0, 120.0, 135.0, 150.0, 179.5]) * np.pi / 180
+    from iterative_tomographic_reconstruction_algorithms_b200.class_projectors_radon import shim_angles
+    plans = [_lib.Plan(_lib.KIND_DD, 300, _angles(250), nz=2), _lib.Plan(_lib.KIND_DD, 97, _angles(61), nz=1),
+             _lib.Plan(_lib.KIND_DD, 48, shim_angles("dd", special.astype(np.float32)), nz=1), _batch()]
+    for p in plans:
+        img = torch.from_numpy(rng.standard_normal(p.image_shape).astype(np.float32)).cuda()
+        sino = torch.from_numpy(rng.standard_normal(p.sino_shape).astype(np.float32)).cuda()
+        p.set_tuning("w2w", "t1")
+        f0, a0 = p.forward(img), p.adjoint(sino)
+        for s in ADJ_SHAPES:
+            p.set_tuning(None, s)
+            assert torch.equal(p.adjoint(sino), a0), (p.image_shape, s)
+        for s in FWD_SHAPES:
+            p.set_tuning(s, None)
+            assert torch.equal(p.forward(img), f0), (p.image_shape, s)
+        assert "set by the caller" in p.tuning()
+        with pytest.raises(ValueError):
+            p.set_tuning(None, "w2w")  # adjoint shapes are t1 / t2 / t4
+
+
+def test_launch_shape_in_fused_solvers(cuda):
+    """The solvers' adjoint epilogues (SIRT update, SPS clip, MLEM) under two adjoint shapes."""
+    torch = cuda
+    from iterative_tomographic_reconstruction_algorithms_b200 import _lib
+    from iterative_tomographic_reconstruction_algorithms_b200.phantom import random_ellipses
+    from iterative_tomographic_reconstruction_algorithms_b200.solvers import Solver
+    n, na = 128, 90
+    x_true = torch.from_numpy(random_ellipses(n, seed=5)).cuda()[None].contiguous()
+    for algo in ("sirt", "sps", "em"):
+        out = []
+        for adj in ("t1", "t4"):
+            p = _lib.Plan(_lib.KIND_DD, n, _angles(na), nz=1)
+            p.set_tuning(None, adj)
+            b = p.forward(x_true)
+            x, res = Solver(p, algo, b).run(torch.ones_like(x_true), 5)
+            out.append((x, res))
+        assert torch.equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1]), algo
