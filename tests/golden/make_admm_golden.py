@@ -3,7 +3,10 @@
 Runs the reference's own solver functions -- algorithms/admm.py conj_grad,
 lasso_l1 and lasso_tv with their inner algorithms/cg.py loops and
 algorithms/utils.py -- imported from the reference tree, over the compiled
-reference dd projector (oracle/_ref, ``make -C oracle ref``).  The plotting,
+reference dd projector (oracle/_ref, ``make -C oracle ref``).  Each case also
+records its noise floor: the relative change of the reference's own result
+when the same solver runs on the float64-accumulating dd oracle instead (only
+the projector's float32 accumulation rounding differs).  The plotting,
 image-IO and projector-class modules those files import but these functions
 do not use are replaced by empty modules, and multiprocessing.Pool by an
 in-process pool (apply_async runs the call at once), as the drop-in package
@@ -23,7 +26,7 @@ ROOT = Path(__file__).resolve().parents[2]
 sys.path.insert(0, str(ROOT))
 REF_ALGOS = Path("/root/reference/algorithms")
 
-from oracle.oracle import RefLib, radon_angles  # noqa: E402
+from oracle.oracle import Oracle, RefLib, radon_angles  # noqa: E402
 from iterative_tomographic_reconstruction_algorithms_b200.phantom import random_ellipses  # noqa: E402
 
 OUT = Path(__file__).resolve().parent
@@ -78,6 +81,18 @@ class RefDD:
         return self.R.radon("dd", 1, np.asarray(y).astype(np.float32), self.ang)
 
 
+class Fp64DD(RefDD):
+    """The same dd geometry and bin decisions, accumulated in float64 (the
+    project's oracle, oracle/tomo_oracle.c), rounded to float32: the reference
+    operator without its float32 accumulation rounding."""
+
+    def A(self, x):
+        return self.R.radon("dd", 0, np.asarray(x).astype(np.float32), self.ang).astype(np.float32)
+
+    def At(self, y):
+        return self.R.radon("dd", 1, np.asarray(y).astype(np.float32), self.ang).astype(np.float32)
+
+
 class RefGrid:
     """class_projectors_grid.projectors(n, angles, kernel='kb', oversampl=1.5, W=6.6, errs=6e-6,
     interp='lin') -- admm.py's 'grid-kb' projector (admm.py:885-887) -- over the compiled reference C."""
@@ -108,6 +123,7 @@ def param_ns(**kw):
 def main() -> None:
     admm = load_reference()
     R = RefLib()
+    O = Oracle()
     rng = np.random.default_rng(20261204)
     data = {}
     cases = [
@@ -143,7 +159,15 @@ def main() -> None:
         data[f"{name}/b"] = b
         data[f"{name}/x"] = np.asarray(x, np.float32)
         data[f"{name}/info"] = np.asarray(info, np.float64)
-        print(name, np.asarray(info)[-1])
+        # noise floor: how far the reference's own result moves when only its
+        # projector's float32 accumulation rounding changes (the same solver on
+        # the float64-accumulating dd oracle); no such oracle for gridding: 0
+        floor = 0.0
+        if not name.startswith("grid"):
+            x64, _ = fn(x0.copy(), b, Fp64DD(O, n, deg), prm)
+            floor = float(np.linalg.norm(np.asarray(x64, np.float64) - x) / np.linalg.norm(np.asarray(x, np.float64)))
+        data[f"{name}/floor"] = np.array([floor])
+        print(name, np.asarray(info)[-1], "floor", floor)
     np.savez_compressed(OUT / "admm_golden.npz", **data)
     print("wrote admm_golden.npz")
 

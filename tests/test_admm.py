@@ -8,11 +8,16 @@ oracle/admm_oracle.py restates those loops; with numpy's inner products it
 reproduces every case bit for bit (CPU test below), which pins the types and
 rounding the kernels follow.
 
-Tolerances (rel L2 of the final image): Lasso-L1 / Lasso-TV 1e-4 (the solver
-bar).  Plain CG 2e-3: its float32 iterate is sensitive to the order of the
-float32 inner products alone -- the oracle with every dot accumulated in
-float64 (the device's choice) already moves it by 4.4e-4 on cg_n48 -- so the
-bar is a few times that spread.
+Tolerances (rel L2 of the final image): max(1e-4, 3 x floor), where each
+case's floor (stored with the fixture) is how far the reference's OWN result
+moves when its projector accumulates in float64 instead of float32, the same
+solver and geometry otherwise.  The well-conditioned cases have floors of
+2e-6 to 7e-6 and keep the 1e-4 solver bar; float32 CG (cg_n48, floor 9.0e-4)
+and Lasso-L1 with a weak L2 term (l1_n48, floor 3.2e-4) amplify rounding of
+1.5e-7 per projector application by three orders of magnitude, so a
+projector that rounds differently from the reference's C -- as any GPU
+accumulation order does -- can only be held to a few times that spread.
+The gridding case has no float64 oracle (floor 0, bar 1e-4).
 """
 from __future__ import annotations
 
@@ -91,12 +96,13 @@ def test_device_solvers_match_reference(cuda, admm_golden):
         x0 = np.ones((c["nz"], c["n"], c["n"]), np.float32)
         x, info = fn[c["reg"]](x0, admm_golden[f"{name}/b"], tp, _param(c))
         assert x is x0  # updated in place, as the reference does
-        tol = 2e-3 if c["reg"] == "cg" else 1e-4
-        assert rel_l2(x, admm_golden[f"{name}/x"]) <= tol, (name, rel_l2(x, admm_golden[f"{name}/x"]))
+        floor = float(admm_golden[f"{name}/floor"][0])
+        tol = max(1e-4, 3.0 * floor)
+        assert rel_l2(x, admm_golden[f"{name}/x"]) <= tol, (name, rel_l2(x, admm_golden[f"{name}/x"]), tol)
         ref_info = admm_golden[f"{name}/info"]
         info = np.asarray(info)
         assert info.shape == ref_info.shape, name
-        itol = 2e-2 if c["reg"] == "cg" else 2e-3
+        itol = 2e-2 if floor > 1e-4 else 2e-3
         for col in (0, 1, 2):
             if c["reg"] == "cg" and col == 1:
                 assert np.all(info[:, 1] == 0.0)
