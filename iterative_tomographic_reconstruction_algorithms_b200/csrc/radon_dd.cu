@@ -148,6 +148,10 @@ __global__ void __launch_bounds__(128) dd_forward_kernel(
 // Instances
 // ---------------------------------------------------------------------------
 constexpr int kGrpDet = 127;              // detectors per forward item (128 boundaries, 4 per lane)
+#ifndef FWD_UNROLL
+#define FWD_UNROLL 2
+#endif
+constexpr int kFwdUnroll = FWD_UNROLL;  // image lines per unrolled step of the forward
 constexpr int kTileW = 32, kTileH = 16;   // pixels per adjoint item (4x4 per lane, 8x4 lanes)
 constexpr int kScanThreads = 256;
 constexpr int kColWarps = 4, kColRows = 16;
@@ -360,19 +364,20 @@ __device__ __forceinline__ void dd_fwd_lines(int ia, int ib, const double2 *__re
                                              const float (&lo_nh)[4], double (&T)[4], double (&C)[4]) {
   float y = (float)(ia - nh) + 0.5f;
   const double2 *sl = SL + (size_t)ia * ws;
-  const float nlim = (float)n + 0.25f, nhf = (float)nh;
-#pragma unroll 2
+  const float nlim = (float)n + 0.25f, cmn = kMagic + (float)nh;
+#pragma unroll kFwdUnroll
   for (int i = ia; i < ib; ++i) {
     const float q = __fmul_rn(y, k);
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
-      // kk = floor(D + nh + q) clamped to [-1, n], as a float and an int by
-      // rounding at 1.5 * 2^23 (an index one off at a pixel boundary leaves F
-      // unchanged up to rounding, F being continuous)
+      // kk = floor(D + nh + q) clamped to [-1, n], as a float and an int:
+      // t + 1.5 * 2^23 rounded down lies where floats are the integers, so
+      // f = 1.5 * 2^23 + floor(t) exactly, and its bits give kk
       const float t = fminf(fmaxf(__fadd_rn(lo_nh[j], q), -0.5f), nlim);
-      const float f = __fadd_rn(__fadd_rn(t, -0.5f), kMagic);
+      const float f = __fadd_rd(t, kMagic);
       const int kk = __float_as_int(f) - kMagicBits;
-      const float Pk = __fsub_rn(__fsub_rn(__fsub_rn(f, kMagic), nhf), q);
+      // P_kk = (kk - nh) - q, with kk - nh = f - (1.5 * 2^23 + nh) exactly
+      const float Pk = __fsub_rn(__fsub_rn(f, cmn), q);
       const double2 e = __ldg(sl + kk);
       T[j] = fma((double)__fsub_rn(Dlo[j], Pk), e.y, T[j] + e.x);
     }
