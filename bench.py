@@ -52,7 +52,7 @@ def parse():
                     help="run only warm-up + steps of the device path (for ncu captures)")
     ap.add_argument("--n", type=int, default=N_SIDE, help="image side (profiling only)")
     ap.add_argument("--na", type=int, default=N_ANG, help="angle count (profiling only)")
-    ap.add_argument("--workload", default="pair", choices=["pair", "batch", "warmstart", "admm"],
+    ap.add_argument("--workload", default="pair", choices=["pair", "batch", "warmstart", "admm", "kinds"],
                     help="pair: the dd pair at 2048^2 x 1800 (default); batch: batched uneven SIRT; "
                          "warmstart: learned warm start, time to the plain SIRT residual")
     ap.add_argument("--train-pairs", type=int, default=256, help="warmstart: training samples")
@@ -62,6 +62,7 @@ def parse():
     ap.add_argument("--slices", type=int, default=64, help="batch workload: number of slices")
     ap.add_argument("--no-cpu-baseline", action="store_true", help="admm workload: skip the host reference sample")
     ap.add_argument("--iters", type=int, default=10, help="batch workload: SIRT iterations per step")
+    ap.add_argument("--kinds", default="pd,rd,dd,ss,bspline,grid", help="kinds workload: projectors to time")
     return ap.parse_args()
 
 
@@ -378,6 +379,84 @@ def run_admm(args, rank, world, local):
     print(json.dumps(out), flush=True)
 
 
+# gathered operand bytes per pixel x angle update of each projector (its reference
+# arithmetic): 4 B x taps read per update; B-spline 5 taps + 5 LUT values
+TAU_BYTES = {"pd": 32.0, "rd": 25.6, "dd": 8.0, "ss": 8.0, "bspline": 40.0}
+
+
+def run_kinds(args, rank, world, local):
+    """Every projector pair through its class API on one seeded random-ellipse
+    slice: pd, rd, dd, ss (class_projectors_radon), cubic B-spline
+    (class_projectors_bspline, radon_degree 1) and gridding (Kaiser-Bessel W=6,
+    os 2, linear interpolation).  Each forward and each adjoint application is
+    timed alone with CUDA events after warm-up, L2 flushed (256 MiB write)
+    before every application; GUPS = n^2 na / time.  For the gather kernels the
+    line also gives the gathered operand bytes per second against the L1 4-byte
+    load rate measured in the same run."""
+    import ctypes
+
+    import torch
+    from iterative_tomographic_reconstruction_algorithms_b200 import _lib
+    from iterative_tomographic_reconstruction_algorithms_b200 import class_projectors_bspline as cpb
+    from iterative_tomographic_reconstruction_algorithms_b200 import class_projectors_grid as cpg
+    from iterative_tomographic_reconstruction_algorithms_b200 import class_projectors_radon as cpr
+    from iterative_tomographic_reconstruction_algorithms_b200.phantom import random_ellipses
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    n, na = args.n, args.na
+    deg = np.linspace(0, 180, na, endpoint=False)
+    s_gbs, l1_gbs, f_tf = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+    _lib.lib.tomo_measure_onchip_peaks.argtypes = [ctypes.POINTER(ctypes.c_double)] * 3
+    _lib.check(_lib.lib.tomo_measure_onchip_peaks(ctypes.byref(s_gbs), ctypes.byref(l1_gbs), ctypes.byref(f_tf)),
+               "onchip peaks")
+    x = torch.from_numpy(random_ellipses(n, seed=0)).to(dev)
+    y = torch.from_numpy(np.random.default_rng(1).standard_normal((na, n)).astype(np.float32)).to(dev)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    out = {}
+    kinds = [k for k in args.kinds.split(",") if k]
+    with ClockSampler(local) as clk:
+        for kind in kinds:
+            if kind in ("pd", "rd", "dd", "ss"):
+                tp = cpr.projectors(n, deg, oper=kind)
+            elif kind == "bspline":
+                tp = cpb.projectors(n, deg, None, bspline_degree=3, proj_support_y=4, radon_degree=1)
+            else:
+                tp = cpg.projectors(n, deg, kernel="kb", oversampl=2.0, W=6.0, errs=1e-3, interp="lin",
+                                    verbose=False)
+            res = {}
+            for name, fn, arg in (("forward", tp.A, x), ("adjoint", tp.At, y)):
+                for _ in range(max(1, args.warmup)):
+                    fn(arg)
+                times = []
+                for _ in range(args.steps):
+                    flush.fill_(1.0)
+                    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    e0.record(stream)
+                    fn(arg)
+                    e1.record(stream)
+                    torch.cuda.synchronize()
+                    times.append(e0.elapsed_time(e1))
+                ms = float(np.median(times))
+                gups = n * n * na / (ms * 1e-3) / 1e9
+                r = {"ms": ms, "gups": gups}
+                if kind in TAU_BYTES:
+                    gbs = TAU_BYTES[kind] * n * n * na / (ms * 1e-3) / 1e9
+                    r["gathered_gbs"] = gbs
+                    r["frac_of_l1"] = gbs / l1_gbs.value
+                res[name] = r
+            out[kind] = res
+            del tp
+            torch.cuda.empty_cache()
+    print(json.dumps({
+        "metric": "per-projector GUPS (pixel x angle updates per second per application)", "unit": "GUPS",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "dtype": "f32",
+        "data": "synthetic", "config": {"workload": f"each projector pair, {n}x{n} image, {na} angles [0,180), {n} bins",
+                                        "l2": "flushed before every application (256 MiB write)"},
+        "kinds": out, "onchip_peaks": {"smem_gbs": s_gbs.value, "l1_gbs": l1_gbs.value, "fp32_tflops": f_tf.value},
+        "clocks": clk.summary()}), flush=True)
+
+
 def admm_cpu_baseline(tp, b0, n, n2):
     """The reference's outer ADMM-TV iteration on the host, extrapolated from one
     forward + adjoint of the compiled reference gridding C (oracle/_ref, with the
@@ -416,6 +495,8 @@ def main():
         return run_warmstart(args, rank, world, local)
     if args.workload == "admm":
         return run_admm(args, rank, world, local)
+    if args.workload == "kinds":
+        return run_kinds(args, rank, world, local)
 
     import torch
     import torch.distributed as dist
