@@ -25,6 +25,8 @@ namespace tomo {
 namespace {
 
 constexpr double kPi = 3.141592653589793;
+constexpr float kPdMagic = 12582912.0f;  // 1.5 * 2^23
+constexpr int kPdMagicBits = 0x4B400000;  // its bit pattern
 
 struct PdEval {
   float wl, wu;  // weights of bins l = floor(T), u = ceil(T)
@@ -38,12 +40,16 @@ __device__ __forceinline__ PdEval pd_eval(float x, float y, const PdAngle &g, fl
   const bool keep = ((g.flags & 1) && y > r) || ((g.flags & 2) && y > r) || ((g.flags & 4) && y > 0.0f);
   const float ts = keep ? t : -t;
   const float T = __fsub_rn(fnh, ts);
-  const float lf = floorf(T), uf = ceilf(T);
+  // floor and ceil of T without the conversion pipe: T + 1.5 * 2^23 rounded
+  // down / up lies where floats are the integers (|T| < 2^22), so it is
+  // 1.5 * 2^23 + floor(T) / ceil(T) exactly, and its bits give the integer
+  const float fd = __fadd_rd(T, kPdMagic), fu = __fadd_ru(T, kPdMagic);
+  const float lf = __fsub_rn(fd, kPdMagic), uf = __fsub_rn(fu, kPdMagic);
   PdEval e;
   e.wl = fabsf(__fsub_rn(__fadd_rn(ts, uf), fnh));
   e.wu = fabsf(__fsub_rn(T, lf));
-  e.l = (lf >= 1.0f && lf < (float)n) ? (int)lf : -1;
-  e.u = (uf >= 1.0f && uf < (float)n) ? (int)uf : -1;
+  e.l = (lf >= 1.0f && lf < (float)n) ? __float_as_int(fd) - kPdMagicBits : -1;
+  e.u = (uf >= 1.0f && uf < (float)n) ? __float_as_int(fu) - kPdMagicBits : -1;
   return e;
 }
 

@@ -70,9 +70,29 @@ __device__ __forceinline__ SubRay rd_subray(float t, const RdAngle &g, int nh) {
   return r;
 }
 
-// alpha of the crossing out of column/row state `idx` (float of a double quotient)
-__device__ __forceinline__ float rd_alpha(int idx, int d, float p, float e) {
-  return __double2float_rn(__ddiv_rn(__dsub_rn(__dadd_rn((double)idx, 0.5 * d), (double)p), (double)e));
+// Numerator of the crossing out of column/row state `idx`: (idx + d/2) - p,
+// exact in double.
+__device__ __forceinline__ double rd_num(int idx, int d, float p) {
+  return __dsub_rn(__dadd_rn((double)idx, 0.5 * d), (double)p);
+}
+
+// alpha = the float of the double quotient num / e, as the reference computes
+// it (one double division, rounded to float).  The product num * re, re the
+// double reciprocal of e, is within 2^-51 (relative) of the correctly rounded
+// quotient Q; if it rounds to the same float after moving it down and up by
+// 2^-49 (relative), that float is Q's.  Otherwise (Q within a hair of a
+// float rounding boundary, e == 0, overflow) the division is done.
+__device__ __forceinline__ float rd_alpha_q(double num, float e, double re) {
+  const double q = __dmul_rn(num, re);
+  const double m = fabs(q) * 0x1p-49;
+  const float lo = __double2float_rn(__dsub_rn(q, m)), hi = __double2float_rn(__dadd_rn(q, m));
+  if (lo == hi) return lo;
+  return __double2float_rn(__ddiv_rn(num, (double)e));
+}
+
+// alpha of the crossing out of column/row state `idx`
+__device__ __forceinline__ float rd_alpha(int idx, int d, float p, float e, double re) {
+  return rd_alpha_q(rd_num(idx, d, p), e, re);
 }
 
 __global__ void __launch_bounds__(128) rd_forward_kernel(
@@ -99,22 +119,30 @@ __global__ void __launch_bounds__(128) rd_forward_kernel(
       const SubRay s = rd_subray(rd_offset(i, n, nh, g.lt, g.gt), g, nh);
       int ii = s.ii0, jj = s.jj0;
       float alpha = 0.0f, alpha_old = 0.0f;
-      float ax = rd_alpha(ii, s.dx, s.p1x, s.ex), ay = rd_alpha(jj, s.dy, s.p1y, s.ey);
+      const double rex = __drcp_rn((double)s.ex), rey = __drcp_rn((double)s.ey);
+      const double ddx = (double)s.dx, ddy = (double)s.dy;
+      // numerators of the next crossings, stepped exactly by +-1
+      double nx = rd_num(ii, s.dx, s.p1x), ny = rd_num(jj, s.dy, s.p1y);
+      float ax = rd_alpha_q(nx, s.ex, rex), ay = rd_alpha_q(ny, s.ey, rey);
       for (int it = 0; alpha <= 1.0f && it < guard; ++it) {
         if (ax < ay) {
           alpha = ax;
           ii += s.dx;
-          ax = rd_alpha(ii, s.dx, s.p1x, s.ex);
+          nx = __dadd_rn(nx, ddx);
+          ax = rd_alpha_q(nx, s.ex, rex);
         } else if (ax > ay) {
           alpha = ay;
           jj += s.dy;
-          ay = rd_alpha(jj, s.dy, s.p1y, s.ey);
+          ny = __dadd_rn(ny, ddy);
+          ay = rd_alpha_q(ny, s.ey, rey);
         } else if (ax == ay) {
           alpha = ay;
           ii += s.dx;
           jj += s.dy;
-          ax = rd_alpha(ii, s.dx, s.p1x, s.ex);
-          ay = rd_alpha(jj, s.dy, s.p1y, s.ey);
+          nx = __dadd_rn(nx, ddx);
+          ny = __dadd_rn(ny, ddy);
+          ax = rd_alpha_q(nx, s.ex, rex);
+          ay = rd_alpha_q(ny, s.ey, rey);
         } else {
           break;  // NaN crossing: the reference would never advance
         }
@@ -182,24 +210,25 @@ __global__ void __launch_bounds__(128) rd_adjoint_kernel(
           const SubRay s = rd_subray(rd_offset(i, n, nh, g.lt, g.gt), g, nh);
           const int A = (iiP - s.ii0) * s.dx, B = (jjP - s.jj0) * s.dy;
           if (A < 0 || B < 0 || (A == 0 && B == 0)) continue;
-          const float XA = rd_alpha(s.ii0 + A * s.dx, s.dx, s.p1x, s.ex);
-          const float YB = rd_alpha(s.jj0 + B * s.dy, s.dy, s.p1y, s.ey);
-          const float XA1 = A >= 1 ? rd_alpha(s.ii0 + (A - 1) * s.dx, s.dx, s.p1x, s.ex) : NEG;
-          const float YB1 = B >= 1 ? rd_alpha(s.jj0 + (B - 1) * s.dy, s.dy, s.p1y, s.ey) : NEG;
+          const double rex = __drcp_rn((double)s.ex), rey = __drcp_rn((double)s.ey);
+          const float XA = rd_alpha(s.ii0 + A * s.dx, s.dx, s.p1x, s.ex, rex);
+          const float YB = rd_alpha(s.jj0 + B * s.dy, s.dy, s.p1y, s.ey, rey);
+          const float XA1 = A >= 1 ? rd_alpha(s.ii0 + (A - 1) * s.dx, s.dx, s.p1x, s.ex, rex) : NEG;
+          const float YB1 = B >= 1 ? rd_alpha(s.jj0 + (B - 1) * s.dy, s.dy, s.p1y, s.ey, rey) : NEG;
           if (!(XA1 < YB && YB1 < XA)) continue;  // state (A, B) never visited
           float ain, aprev;
           if (XA1 > YB1) {  // entered by an x step from (A-1, B)
             ain = XA1;
-            const float XA2 = A >= 2 ? rd_alpha(s.ii0 + (A - 2) * s.dx, s.dx, s.p1x, s.ex) : 0.0f;
+            const float XA2 = A >= 2 ? rd_alpha(s.ii0 + (A - 2) * s.dx, s.dx, s.p1x, s.ex, rex) : 0.0f;
             aprev = fmaxf(XA2, B >= 1 ? YB1 : 0.0f);
           } else if (YB1 > XA1) {  // y step from (A, B-1)
             ain = YB1;
-            const float YB2 = B >= 2 ? rd_alpha(s.jj0 + (B - 2) * s.dy, s.dy, s.p1y, s.ey) : 0.0f;
+            const float YB2 = B >= 2 ? rd_alpha(s.jj0 + (B - 2) * s.dy, s.dy, s.p1y, s.ey, rey) : 0.0f;
             aprev = fmaxf(A >= 1 ? XA1 : 0.0f, YB2);
           } else {  // diagonal step from (A-1, B-1)
             ain = XA1;
-            const float XA2 = A >= 2 ? rd_alpha(s.ii0 + (A - 2) * s.dx, s.dx, s.p1x, s.ex) : 0.0f;
-            const float YB2 = B >= 2 ? rd_alpha(s.jj0 + (B - 2) * s.dy, s.dy, s.p1y, s.ey) : 0.0f;
+            const float XA2 = A >= 2 ? rd_alpha(s.ii0 + (A - 2) * s.dx, s.dx, s.p1x, s.ex, rex) : 0.0f;
+            const float YB2 = B >= 2 ? rd_alpha(s.jj0 + (B - 2) * s.dy, s.dy, s.p1y, s.ey, rey) : 0.0f;
             aprev = fmaxf(XA2, YB2);
           }
           if (!(aprev <= 1.0f)) continue;  // the walk had already stopped
