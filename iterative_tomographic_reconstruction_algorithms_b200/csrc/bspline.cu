@@ -11,11 +11,14 @@
 // lut[angle][li].  ds = (int)(support/2 + 0.5), lut_step = (lut_size/2) /
 // (support/2).  The table itself is built on the host (bspline_functions.py).
 //
-// Forward = gather per (angle, bin) over the strip of pixels whose taps can
-// reach the bin; adjoint = gather per pixel over angles and taps.  Output rows
-// follow the angle order (no reversal).
+// Forward = per (angle, block of bins) a pass over the band of pixels whose
+// taps can reach the bins, summed exactly in fixed point; adjoint = gather
+// per pixel over angles and taps.  Output rows follow the angle order (no
+// reversal).
+#include <algorithm>
 #include <cmath>
 
+#include "fixed_sum.cuh"
 #include "tomo_internal.cuh"
 
 namespace tomo {
@@ -33,36 +36,80 @@ __device__ __forceinline__ int bs_bin(int s, float ps, double mid) {
   return (int)__dadd_rn((double)__fadd_rn((float)s, ps), mid);  // trunc toward zero
 }
 
+
+// Forward: a block owns kBsBins consecutive bins of one angle and slice.  Its
+// warps walk the band of pixels whose taps can reach those bins (a line per
+// warp, each pixel once) and add every tap's product lut * value, as the
+// reference rounds it, into shared-memory bins summed exactly in fixed point
+// (fixed_sum.cuh): deterministic, each bin the exact sum of the reference's
+// float products rounded once.  At most 3 pixels per line and tap reach a bin
+// (ps moves by at least 1/sqrt(2) per pixel), which bounds the sums.
+constexpr int kBsBins = 128, kBsThreads = 256;
+
+
+// LUT index trunc((yi - n/2 - ps) * lut_step) + lut_size/2 (gen_forwproj.c:61).
 __device__ __forceinline__ int bs_lut(int yi, float ps, const BsConst &k) {
   const float y = __fsub_rn((float)yi, k.fmid);
   return (int)__fmul_rn(__fsub_rn(y, ps), k.lut_step) + k.lut_half;
 }
 
-__global__ void __launch_bounds__(128) bs_forward_kernel(
+// The same index with the truncation toward zero taken without the
+// conversion pipe (the forward's inner loop is conversion-bound).
+__device__ __forceinline__ int bs_lut_fast(int yi, float ps, const BsConst &k) {
+  const float a = __fmul_rn(__fsub_rn(__fsub_rn((float)yi, k.fmid), ps), k.lut_step);
+  float fl;
+  const int t = floor_i(fabsf(a), fl);
+  return (a < 0.0f ? -t : t) + k.lut_half;
+}
+
+// bs_bin for even n >= 4 without the conversion pipe: n/2 is an integer, so
+// trunc((double)t + n/2) == floor(t) + n/2, except that t in (-n/2 - 1, -n/2)
+// truncates to bin 0 and a tiny negative t may round up to n/2 in the double
+// sum (t in (-1, 0) takes the double rule).  Odd n: the double rule.
+__device__ __forceinline__ int bs_bin_fast(int s, float ps, const BsConst &k, bool even, int nh, float b0lo) {
+  const float t = __fadd_rn((float)s, ps);
+  if (even && !(t < 0.0f && t > -1.0f)) {
+    float fl;
+    int yi = floor_i(t, fl) + nh;
+    if (yi == -1 && t > b0lo) yi = 0;
+    return yi;
+  }
+  return bs_bin(s, ps, k.mid);
+}
+
+
+__global__ void __launch_bounds__(kBsThreads) bs_forward_kernel(
     const float *__restrict__ img, float *__restrict__ sino, const float2 *__restrict__ cs,
-    const float *__restrict__ lut, BsConst k, FwdEpi ep) {
-  const int b = blockIdx.x * blockDim.x + threadIdx.x;
-  const int v = blockIdx.y;
+    const float *__restrict__ lut, const unsigned *__restrict__ vmax, float lutmax, BsConst k, FwdEpi ep) {
+  extern __shared__ float slut[];  // this angle's lut row
+  __shared__ unsigned long long acc[kBsBins];
+  const int B0 = blockIdx.x * kBsBins, v = blockIdx.y;
   const size_t z = blockIdx.z;
   const int n = k.n;
-  const bool live = b < n;
+  const float *L = lut + (size_t)v * k.lut_size;
+  for (int i = threadIdx.x; i < k.lut_size; i += blockDim.x) slut[i] = __ldg(L + i);
+  for (int i = threadIdx.x; i < kBsBins; i += blockDim.x) acc[i] = 0ull;
+  // fixed-point unit: |bin| <= 3 n (2 ds + 1) max|lut| max|value|
+  const float vm = __uint_as_float(vmax[z]);
+  const FixedScale fs = fixed_scale(3.0 * n * (2.0 * k.ds + 1.0) * (double)lutmax * (double)vm);
+  __syncthreads();
   const float C = cs[v].x, S = cs[v].y;
   const float *I = img + z * (size_t)n * n;
-  const float *L = lut + (size_t)v * k.lut_size;
   const bool by_rows = fabsf(C) >= fabsf(S);  // along a row ps moves by C per pixel
-  // taps reach bin b when b <= ps + s + mid < b + 1 (b = 0 also takes (-1, 0))
-  const float plo = (float)(b - k.ds - 2) - k.fmid, phi = (float)(b + k.ds + 2) - k.fmid;
+  const int Bend = min(B0 + kBsBins, n);
+  const float plo = (float)(B0 - k.ds - 2) - k.fmid, phi = (float)(Bend - 1 + k.ds + 2) - k.fmid;
   const bool even = (n & 1) == 0 && n >= 4;  // n = 2: the bin-0 boundary sits at 0, use the double rule
-  const float bm = (float)b - k.fmid, fds = (float)k.ds;  // b - n/2 (exact for even n)
-  const float b0lo = -k.fmid - 1.0f, b0hi = -k.fmid + 1.0f;
-  float acc = 0.0f;
-  for (int line = 0; line < (live ? n : 0); ++line) {
+  const float b0lo = -k.fmid - 1.0f;
+  const int nh = n / 2;
+  // each warp takes every 8th line, its lanes the line's band of pixels
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int line = warp; line < n; line += kBsThreads / 32) {
     // by rows: ky fixed, ps = kx*C + S*ky; by columns: kx fixed, ps = ky*S + kx*C
     const float fixed = by_rows ? (float)(-line + k.mid) : (float)(line - k.mid);
     const float slope = by_rows ? C : S;
     const float base = by_rows ? S * fixed : C * fixed;
     float u0 = (plo - base) / slope, u1 = (phi - base) / slope;
-    if (u0 > u1) { float t = u0; u0 = u1; u1 = t; }
+    if (u0 > u1) { const float t = u0; u0 = u1; u1 = t; }
     int j0, j1;
     if (by_rows) {  // kx = kx_i - mid
       j0 = (int)floorf(u0 + k.fmid) - 1;
@@ -73,50 +120,27 @@ __global__ void __launch_bounds__(128) bs_forward_kernel(
     }
     j0 = max(j0, 0);
     j1 = min(j1, n - 1);
-    for (int j = j0; j <= j1; ++j) {
+    for (int j = j0 + lane; j <= j1; j += 32) {
       const int kyi = by_rows ? line : j, kxi = by_rows ? j : line;
+      const float val = __ldg(I + (size_t)kyi * n + kxi);
+      if (val == 0.0f) continue;  // adds exactly nothing
       const float ky = (float)(-kyi + k.mid), kx = (float)(kxi - k.mid);
       const float ps = __fmaf_rn(kx, C, __fmul_rn(S, ky));
-      // the tap that lands in bin b: s0 = b - floor(ps + n/2), or a neighbour
-      // of it where the rounding of s + ps crosses an integer (or, for bin 0,
-      // where truncation folds (-1, 0) onto 0); each is checked with the exact
-      // bin rule, so the set of taps is the reference's
-      if (even) {
-        // n/2 is an integer: trunc((double)fl(s + ps) + n/2) == b reduces to
-        // floor(fl(s + ps)) == b - n/2 for b >= 1 and to fl(s + ps) in
-        // (-n/2 - 1, -n/2 + 1) for b = 0, exact in float (checked against the
-        // double rule on CPU for n = 4..4096, including floats next to integers)
-        const float s0 = __fsub_rn(bm, floorf(ps));
-        const float slo = fmaxf(__fsub_rn(s0, b == 0 ? 2.0f : 1.0f), -fds), shi = fminf(__fadd_rn(s0, 1.0f), fds);
-        if (slo > shi) continue;
-        const float val = __ldg(I + (size_t)kyi * n + kxi);
-        for (float sf = slo; sf <= shi; sf = __fadd_rn(sf, 1.0f)) {
-          const float t = __fadd_rn(sf, ps);
-          // (b = n/2: a tiny negative t rounds up to n/2 in the double sum)
-          const bool hit = b == 0 ? (t > b0lo && t < b0hi)
-                                  : (floorf(t) == bm ||
-                                     (bm == 0.0f && t < 0.0f && (int)__dadd_rn((double)t, k.mid) == b));
-          if (!hit) continue;
-          const int li = bs_lut(b, ps, k);
-          if (li >= k.lut_max || li < 0) continue;
-          acc = fmaf(__ldg(L + li), val, acc);
-        }
-        continue;
-      }
-      const int s0 = b - (int)floor(__dadd_rn((double)ps, k.mid));
-      const int slo = max(s0 - (b == 0 ? 2 : 1), -k.ds), shi = min(s0 + 1, k.ds);
-      if (slo > shi) continue;
-      const float val = __ldg(I + (size_t)kyi * n + kxi);
-      for (int s = slo; s <= shi; ++s) {
-        const int yi = bs_bin(s, ps, k.mid);
-        if (yi != b) continue;
-        const int li = bs_lut(yi, ps, k);
+      for (int s = -k.ds; s <= k.ds; ++s) {
+        const int yi = bs_bin_fast(s, ps, k, even, nh, b0lo);
+        if (yi < B0 || yi >= Bend) continue;
+        const int li = bs_lut_fast(yi, ps, k);
         if (li >= k.lut_max || li < 0) continue;
-        acc = fmaf(__ldg(L + li), val, acc);
+        atomicAdd(acc + (yi - B0), fixed_of(__fmul_rn(slut[li], val), fs));
       }
     }
   }
-  fwd_store(ep, acc, live, z * (size_t)k.na * n + (size_t)v * n + (live ? b : 0), sino);
+  __syncthreads();
+  const int b = B0 + (int)threadIdx.x;
+  const bool live = threadIdx.x < kBsBins && b < n;
+  float out = 0.0f;
+  if (live) out = fixed_to_float(acc[threadIdx.x], fs);
+  fwd_store(ep, out, live, z * (size_t)k.na * n + (size_t)v * n + (live ? b : 0), sino);
 }
 
 constexpr int kBsChunk = 1024;
@@ -171,6 +195,17 @@ BsConst make_const(const Plan &p) {
   return k;
 }
 
+struct BsState {
+  float lutmax = 0.0f;        // max |lut|
+  unsigned *vmax = nullptr;   // per slice: max |image| as float bits
+};
+
+void bs_state_free(void *q) {
+  auto *st = (BsState *)q;
+  cudaFree(st->vmax);
+  delete st;
+}
+
 }  // namespace
 
 int bs_setup(Plan &p) {
@@ -191,15 +226,32 @@ int bs_setup(Plan &p) {
   const size_t lb = sizeof(float) * (size_t)na * p.g.lut_size;
   TOMO_CUDA(cudaMalloc(&p.d_aux, lb));
   TOMO_CUDA(cudaMemcpy(p.d_aux, p.g.lut, lb, cudaMemcpyHostToDevice));
+  if (sizeof(float) * (size_t)p.g.lut_size > 200 * 1024)
+    return fail(TOMO_EINVAL, "bspline: lut_size too large (one row must fit in shared memory)");
+  auto *st = new BsState();
+  p.ext = st;
+  p.ext_free = bs_state_free;
+  for (size_t i = 0; i < (size_t)na * p.g.lut_size; ++i) st->lutmax = std::max(st->lutmax, std::fabs(p.g.lut[i]));
+  TOMO_CUDA(cudaMalloc(&st->vmax, sizeof(unsigned) * (size_t)std::max(1, p.g.nz)));
+  if (sizeof(float) * (size_t)p.g.lut_size > 48 * 1024)
+    TOMO_CUDA(cudaFuncSetAttribute(bs_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)(sizeof(float) * (size_t)p.g.lut_size)));
+  // residual partials of the fused solvers: one per warp of the forward launch
+  p.fwd_warps = (size_t)((p.g.n + kBsBins - 1) / kBsBins) * (kBsThreads / 32) * na * p.g.nz;
   p.g.lut = nullptr;
   return TOMO_OK;
 }
 
 int bs_forward(Plan &p, const float *d_img, float *d_sino, cudaStream_t s, const FwdEpi &ep) {
   const BsConst k = make_const(p);
-  dim3 fb(128), fg((k.n + 127) / 128, k.na, p.g.nz);
-  bs_forward_kernel<<<fg, fb, 0, s>>>(d_img, d_sino, (const float2 *)p.d_angles,
-                                      (const float *)p.d_aux, k, ep);
+  BsState &st = *(BsState *)p.ext;
+  const size_t per = (size_t)k.n * k.n;
+  TOMO_CUDA(cudaMemsetAsync(st.vmax, 0, sizeof(unsigned) * p.g.nz, s));
+  fixed_absmax_kernel<<<dim3((unsigned)std::min<size_t>((per + 255) / 256, 1184), p.g.nz), 256, 0, s>>>(d_img, per,
+                                                                                                   st.vmax);
+  dim3 fg((k.n + kBsBins - 1) / kBsBins, k.na, p.g.nz);
+  bs_forward_kernel<<<fg, kBsThreads, sizeof(float) * k.lut_size, s>>>(
+      d_img, d_sino, (const float2 *)p.d_angles, (const float *)p.d_aux, st.vmax, st.lutmax, k, ep);
   TOMO_CUDA(cudaGetLastError());
   return TOMO_OK;
 }

@@ -14,11 +14,14 @@
 // x86-64 code), reproduced exactly: t = |fma(-c, y, x*s)|, the sign test uses
 // (x*s) * (1/c), and the first weight is |(t + ceil(T)) - nh|.
 //
-// Forward = gather per (angle, bin) over the image strip whose sub-samples land
-// within one bin of it; adjoint = gather per pixel over angles.  The duplicate
-// sub-samples are evaluated once with weight 2 * 1/4.
+// Forward = per (angle, block of bins) a pass over the band of pixels whose
+// sub-samples land in the bins, summed exactly in fixed point; adjoint =
+// gather per pixel over angles.  The duplicate sub-samples are evaluated once
+// with weight 2 * 1/4.
+#include <algorithm>
 #include <cmath>
 
+#include "fixed_sum.cuh"
 #include "tomo_internal.cuh"
 
 namespace tomo {
@@ -53,57 +56,68 @@ __device__ __forceinline__ PdEval pd_eval(float x, float y, const PdAngle &g, fl
   return e;
 }
 
-// Forward: thread per (bin b, angle v, slice).  Iterates the lines of the
-// axis along which the projection moves fastest, and per line only the pixels
-// whose sub-samples can land in (b-1, b+1).
-__global__ void __launch_bounds__(128) pd_forward_kernel(
+// Forward: a block owns kPdBins consecutive bins of one angle and slice; its
+// warps walk the band of pixels whose sub-samples can land in (B0 - 1, Bend)
+// (a line per warp, each pixel once, along the axis on which T moves fastest)
+// and add 0.5 w value for every sub-sample and bin into shared-memory bins
+// summed exactly in fixed point (fixed_sum.cuh): deterministic, each bin the
+// exact sum of its float products rounded once.  Per line and sub-sample at
+// most 3 pixels reach a bin (T moves by at least 1/sqrt(2) per pixel), so a
+// bin is bounded by 2 (sub-samples) x 3 n x 0.5 x max|image|.
+constexpr int kPdBins = 128, kPdThreads = 256;
+
+__global__ void __launch_bounds__(kPdThreads) pd_forward_kernel(
     const float *__restrict__ img, float *__restrict__ sino, const PdAngle *__restrict__ tab,
-    int n, int nh, int na, FwdEpi ep) {
-  const int b = blockIdx.x * blockDim.x + threadIdx.x;
-  const int v = blockIdx.y;
+    int n, int nh, int na, const unsigned *__restrict__ vmax, FwdEpi ep) {
+  __shared__ unsigned long long acc[kPdBins];
+  const int B0 = blockIdx.x * kPdBins, v = blockIdx.y;
   const size_t z = blockIdx.z;
-  const bool live = b < n;
+  for (int i = threadIdx.x; i < kPdBins; i += blockDim.x) acc[i] = 0ull;
+  const FixedScale fs = fixed_scale(3.0 * n * (double)__uint_as_float(vmax[z]));
+  __syncthreads();
   const PdAngle g = tab[v];
   const float *I = img + z * (size_t)n * n;
   const float fnh = (float)nh;
-  float acc = 0.0f;
-  if (live && b >= 1) {
-    // T ~ nh - sigma*((y0+d) c - (x0+d) s), sigma = sign(c)
-    const float sg = g.c >= 0.0f ? 1.0f : -1.0f;
-    const bool by_rows = fabsf(g.s) >= fabsf(g.c);
-    for (int line = 0; line < n; ++line) {
-      const float o0 = (float)line - fnh + 0.5f;  // y0 (rows) or x0 (columns)
-      float lo = 1e30f, hi = -1e30f;
+  const int Bend = min(B0 + kPdBins, n);
+  // T ~ nh - sigma*((y0+d) c - (x0+d) s), sigma = sign(c)
+  const float sg = g.c >= 0.0f ? 1.0f : -1.0f;
+  const bool by_rows = fabsf(g.s) >= fabsf(g.c);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int line = warp; line < n; line += kPdThreads / 32) {
+    const float o0 = (float)line - fnh + 0.5f;  // y0 (rows) or x0 (columns)
+    float lo = 1e30f, hi = -1e30f;
+    for (int e = 0; e < 2; ++e) {
+      const float d = e ? 0.25f : -0.25f;
+      for (int f = 0; f < 2; ++f) {
+        const float T = (float)(f ? Bend : B0 - 1);
+        float w;  // the other pixel-centre coordinate giving this T
+        if (by_rows) w = (T - fnh + sg * ((o0 + d) * g.c)) / (sg * g.s) - d;
+        else w = (fnh - T + sg * ((o0 + d) * g.s)) / (sg * g.c) - d;
+        lo = fminf(lo, w);
+        hi = fmaxf(hi, w);
+      }
+    }
+    int j0 = (int)floorf(lo + fnh - 0.5f) - 1, j1 = (int)ceilf(hi + fnh - 0.5f) + 1;
+    j0 = max(j0, 0);
+    j1 = min(j1, n - 1);
+    for (int j = j0 + lane; j <= j1; j += 32) {
+      const int ii = by_rows ? line : j, jj = by_rows ? j : line;
+      const float val = __ldg(I + (size_t)(n - 1 - ii) * n + jj);
+      if (val == 0.0f) continue;  // adds exactly nothing
+      const float x0 = (float)jj - fnh + 0.5f, y0 = (float)ii - fnh + 0.5f;
       for (int e = 0; e < 2; ++e) {
         const float d = e ? 0.25f : -0.25f;
-        for (int f = 0; f < 2; ++f) {
-          const float T = (float)(b - 1 + 2 * f);
-          float w;  // the other pixel-centre coordinate giving this T
-          if (by_rows) w = (T - fnh + sg * ((o0 + d) * g.c)) / (sg * g.s) - d;
-          else w = (fnh - T + sg * ((o0 + d) * g.s)) / (sg * g.c) - d;
-          lo = fminf(lo, w);
-          hi = fmaxf(hi, w);
-        }
-      }
-      int j0 = (int)floorf(lo + fnh - 0.5f) - 1, j1 = (int)ceilf(hi + fnh - 0.5f) + 1;
-      j0 = max(j0, 0);
-      j1 = min(j1, n - 1);
-      for (int j = j0; j <= j1; ++j) {
-        const int ii = by_rows ? line : j, jj = by_rows ? j : line;
-        const float x0 = (float)jj - fnh + 0.5f, y0 = (float)ii - fnh + 0.5f;
-        const float val = __ldg(I + (size_t)(n - 1 - ii) * n + jj);
-        float wsum = 0.0f;
-        for (int e = 0; e < 2; ++e) {
-          const float d = e ? 0.25f : -0.25f;
-          const PdEval q = pd_eval(__fadd_rn(x0, d), __fadd_rn(y0, d), g, fnh, n);
-          if (q.l == b) wsum += q.wl;
-          if (q.u == b) wsum += q.wu;
-        }
-        if (wsum != 0.0f) acc = fmaf(0.5f * wsum, val, acc);
+        const PdEval q = pd_eval(__fadd_rn(x0, d), __fadd_rn(y0, d), g, fnh, n);
+        if (q.l >= B0 && q.l < Bend) atomicAdd(acc + (q.l - B0), fixed_of(__fmul_rn(0.5f * q.wl, val), fs));
+        if (q.u >= B0 && q.u < Bend) atomicAdd(acc + (q.u - B0), fixed_of(__fmul_rn(0.5f * q.wu, val), fs));
       }
     }
   }
-  fwd_store(ep, acc, live, z * (size_t)na * n + (size_t)v * n + (live ? b : 0), sino);
+  __syncthreads();
+  const int b = B0 + (int)threadIdx.x;
+  const bool live = threadIdx.x < kPdBins && b < n;
+  const float out = live ? fixed_to_float(acc[threadIdx.x], fs) : 0.0f;
+  fwd_store(ep, out, live, z * (size_t)na * n + (size_t)v * n + (live ? b : 0), sino);
 }
 
 constexpr int kPdChunk = 1024;
@@ -163,13 +177,22 @@ int pd_setup(Plan &p) {
   }
   TOMO_CUDA(cudaMalloc(&p.d_angles, sizeof(PdAngle) * (size_t)na));
   TOMO_CUDA(cudaMemcpy(p.d_angles, tab.data(), sizeof(PdAngle) * (size_t)na, cudaMemcpyHostToDevice));
+  // per-slice max |image| of the forward's fixed-point sums
+  TOMO_CUDA(cudaMalloc(&p.ext, sizeof(unsigned) * (size_t)std::max(1, p.g.nz)));
+  p.ext_free = [](void *q) { cudaFree(q); };
+  // residual partials of the fused solvers: one per warp of the forward launch
+  p.fwd_warps = (size_t)((p.g.n + kPdBins - 1) / kPdBins) * (kPdThreads / 32) * na * p.g.nz;
   return TOMO_OK;
 }
 
 int pd_forward(Plan &p, const float *d_img, float *d_sino, cudaStream_t s, const FwdEpi &ep) {
   const int n = p.g.n, na = p.g.na, nz = p.g.nz;
-  dim3 fb(128), fg((n + 127) / 128, na, nz);
-  pd_forward_kernel<<<fg, fb, 0, s>>>(d_img, d_sino, (const PdAngle *)p.d_angles, n, p.nh, na, ep);
+  unsigned *vmax = (unsigned *)p.ext;
+  const size_t per = (size_t)n * n;
+  TOMO_CUDA(cudaMemsetAsync(vmax, 0, sizeof(unsigned) * nz, s));
+  fixed_absmax_kernel<<<dim3((unsigned)std::min<size_t>((per + 255) / 256, 1184), nz), 256, 0, s>>>(d_img, per, vmax);
+  dim3 fg((n + kPdBins - 1) / kPdBins, na, nz);
+  pd_forward_kernel<<<fg, kPdThreads, 0, s>>>(d_img, d_sino, (const PdAngle *)p.d_angles, n, p.nh, na, vmax, ep);
   TOMO_CUDA(cudaGetLastError());
   return TOMO_OK;
 }
