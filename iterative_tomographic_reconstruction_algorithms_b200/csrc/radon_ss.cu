@@ -21,6 +21,7 @@
 #include <algorithm>
 #include <cmath>
 
+#include "fixed_sum.cuh"
 #include "tomo_internal.cuh"
 
 namespace tomo {
@@ -67,9 +68,9 @@ __global__ void __launch_bounds__(128) ss_forward_kernel(
     const int mm = m + nh;
     if (mm < 0 || mm > n - 1) continue;
     const float f = __fmul_rn(__fmaf_rn(-(float)m, g.a, ft), g.rb);
-    const float fl = floorf(f);
+    float fl;
+    const int q = floor_i(f, fl) + nh;
     const float w = __fsub_rn(f, fl), w1 = __fsub_rn(__fadd_rn(fl, 1.0f), f);
-    const int q = (int)fl + nh;
     const float *row = M + (size_t)mm * n;
     if (q >= 0 && q <= n - 1) acc = fmaf(g.wt * w1, __ldg(row + q), acc);
     if (q + 1 >= 0 && q + 1 <= n - 1) acc = fmaf(g.wt * w, __ldg(row + q + 1), acc);
@@ -80,13 +81,14 @@ __global__ void __launch_bounds__(128) ss_forward_kernel(
 // Adjoint: one thread per output pixel, all angles in order.  For the pixel
 // (row R, column C) and an angle, the rays that touch it are those whose
 // minor coordinate lands in [C' - 1, C' + 1) at the pixel's major coordinate;
-// 1 to 3 candidate t per angle are checked with the forward arithmetic.
+// at most 3 candidate t per angle are checked with the forward arithmetic.
 constexpr int kSsChunk = 512;
 
 __global__ void __launch_bounds__(256) ss_adjoint_kernel(
     const float *__restrict__ sino, float *__restrict__ img, const SsAngle *__restrict__ tab,
     const int2 *__restrict__ lim, int n, int nh, int na, AdjEpi ep) {
   __shared__ SsAngle stab[kSsChunk];
+  __shared__ float cbs[kSsChunk];  // 1 / rb (cos or sin)
   const int C = blockIdx.x * blockDim.x + threadIdx.x;
   const int R = blockIdx.y * blockDim.y + threadIdx.y;
   const size_t z = blockIdx.z;
@@ -98,7 +100,10 @@ __global__ void __launch_bounds__(256) ss_adjoint_kernel(
   for (int v0 = 0; v0 < na; v0 += kSsChunk) {
     const int cnt = min(kSsChunk, na - v0);
     __syncthreads();
-    for (int t = tid; t < cnt; t += nthr) stab[t] = tab[v0 + t];
+    for (int t = tid; t < cnt; t += nthr) {
+      stab[t] = tab[v0 + t];
+      cbs[t] = 1.0f / tab[v0 + t].rb;
+    }
     __syncthreads();
     if (!live) continue;
     for (int u = 0; u < cnt; ++u) {
@@ -107,12 +112,15 @@ __global__ void __launch_bounds__(256) ss_adjoint_kernel(
       // major coordinate m and minor index of this pixel
       const int m = g.steep ? R - nh : C - nh;
       const int minor = g.steep ? C : R;
-      // f(t) = fma(-m, a, t) * rb ~ (t - m a) rb must land in [minor-nh-1, minor-nh+1)
+      // f(t) = fma(-m, a, t) * rb ~ (t - m a) rb must land in [minor-nh-1, minor-nh+1):
+      // t in [ta, tb] up to rounding (below 1e-3 here), so the integers in
+      // [ta - 0.01, tb + 0.01] are the candidates (at most 3: |rb| >= 1)
       const float ma = (float)m * g.a;
       const float lo = (float)(minor - nh - 1), hi = (float)(minor - nh + 1);
-      float ta = lo / g.rb + ma, tb = hi / g.rb + ma;
+      float ta = fmaf(lo, cbs[u], ma), tb = fmaf(hi, cbs[u], ma);
       if (ta > tb) { float x = ta; ta = tb; tb = x; }
-      int t0 = (int)floorf(ta) - 1, t1 = (int)ceilf(tb) + 1;
+      float fl0, fl1;
+      int t0 = floor_i(ta - 0.01f, fl0) + 1, t1 = floor_i(tb + 0.01f, fl1);
       t0 = max(t0, -nh);
       t1 = min(t1, nh - 1);
       const float *row = S + (size_t)g.out_row * n;
@@ -121,8 +129,8 @@ __global__ void __launch_bounds__(256) ss_adjoint_kernel(
         const int2 L = __ldg(lrow + t + nh);
         if (m < L.x || m >= L.y) continue;
         const float f = __fmul_rn(__fmaf_rn(-(float)m, g.a, (float)t), g.rb);
-        const float fl = floorf(f);
-        const int q = (int)fl + nh;
+        float fl;
+        const int q = floor_i(f, fl) + nh;
         float wgt;
         if (q == minor) wgt = __fsub_rn(__fadd_rn(fl, 1.0f), f);
         else if (q + 1 == minor) wgt = __fsub_rn(f, fl);
