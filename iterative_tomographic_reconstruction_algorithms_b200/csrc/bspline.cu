@@ -131,7 +131,7 @@ __global__ void __launch_bounds__(kBsThreads) bs_forward_kernel(
         if (yi < B0 || yi >= Bend) continue;
         const int li = bs_lut_fast(yi, ps, k);
         if (li >= k.lut_max || li < 0) continue;
-        atomicAdd(acc + (yi - B0), fixed_of(__fmul_rn(slut[li], val), fs));
+        fixed_add(acc + (yi - B0), fixed_of(__fmul_rn(slut[li], val), fs));
       }
     }
   }

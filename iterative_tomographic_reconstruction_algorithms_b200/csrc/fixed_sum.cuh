@@ -46,6 +46,18 @@ __device__ __forceinline__ unsigned long long fixed_of(float p, const FixedScale
   return (unsigned long long)__float2ll_rn(__fmul_rn(__fmul_rn(p, f.s1), f.s2));
 }
 
+// Adds v to the 64-bit shared-memory sum *a with 32-bit atomics: the low word
+// first, then (high word of v + the carry out of the low word) to the high
+// word, skipped when zero.  After all adds the pair holds the sum mod 2^64
+// whatever the order (every carry is counted once).
+__device__ __forceinline__ void fixed_add(unsigned long long *a, unsigned long long v) {
+  unsigned *w = (unsigned *)a;  // little-endian: w[0] low, w[1] high
+  const unsigned lo = (unsigned)v, hi = (unsigned)(v >> 32);
+  const unsigned old = atomicAdd(w, lo);
+  const unsigned h = hi + ((unsigned)(old + lo) < old ? 1u : 0u);
+  if (h) atomicAdd(w + 1, h);
+}
+
 __device__ __forceinline__ float fixed_to_float(unsigned long long a, const FixedScale &f) {
   return (float)ldexp((double)(long long)a, -f.E);
 }

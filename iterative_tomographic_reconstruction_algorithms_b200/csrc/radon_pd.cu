@@ -108,8 +108,8 @@ __global__ void __launch_bounds__(kPdThreads) pd_forward_kernel(
       for (int e = 0; e < 2; ++e) {
         const float d = e ? 0.25f : -0.25f;
         const PdEval q = pd_eval(__fadd_rn(x0, d), __fadd_rn(y0, d), g, fnh, n);
-        if (q.l >= B0 && q.l < Bend) atomicAdd(acc + (q.l - B0), fixed_of(__fmul_rn(0.5f * q.wl, val), fs));
-        if (q.u >= B0 && q.u < Bend) atomicAdd(acc + (q.u - B0), fixed_of(__fmul_rn(0.5f * q.wu, val), fs));
+        if (q.l >= B0 && q.l < Bend) fixed_add(acc + (q.l - B0), fixed_of(__fmul_rn(0.5f * q.wl, val), fs));
+        if (q.u >= B0 && q.u < Bend) fixed_add(acc + (q.u - B0), fixed_of(__fmul_rn(0.5f * q.wu, val), fs));
       }
     }
   }
