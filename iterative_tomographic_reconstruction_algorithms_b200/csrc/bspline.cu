@@ -157,6 +157,8 @@ __global__ void __launch_bounds__(256) bs_adjoint_kernel(
   const float *Sg = sino + z * (size_t)k.na * n;
   const int tid = threadIdx.y * blockDim.x + threadIdx.x, nthr = blockDim.x * blockDim.y;
   const float ky = (float)(-kyi + k.mid), kx = (float)(kxi - k.mid);
+  const bool even = (n & 1) == 0 && n >= 4;
+  const int nh = n / 2;
   float acc = 0.0f;
   for (int v0 = 0; v0 < k.na; v0 += kBsChunk) {
     const int cnt = min(kBsChunk, k.na - v0);
@@ -169,6 +171,23 @@ __global__ void __launch_bounds__(256) bs_adjoint_kernel(
       const float ps = __fmaf_rn(kx, scs[u].x, __fmul_rn(scs[u].y, ky));
       const float *row = Sg + (size_t)v * n;
       const float *L = lut + (size_t)v * k.lut_size;
+      float fl;
+      const int base = floor_i(ps, fl);
+      const float frac = __fsub_rn(ps, fl);
+      if (even && frac >= 0x1p-12f && frac <= 1.0f - 0x1p-12f) {
+        // ps is at least 2^-12 from an integer, so fl(s + ps) never rounds
+        // across one: every tap's bin is floor(ps) + s + n/2, with the
+        // reference's truncation folding -1 onto bin 0 (t in (-n/2 - 1, -n/2))
+        for (int s = -k.ds; s <= k.ds; ++s) {
+          int yi = base + s + nh;
+          if (yi == -1) yi = 0;
+          if (yi >= n || yi < 0) continue;
+          const int li = bs_lut(yi, ps, k);
+          if (li >= k.lut_max || li < 0) continue;
+          acc = fmaf(__ldg(row + yi), __ldg(L + li), acc);
+        }
+        continue;
+      }
       for (int s = -k.ds; s <= k.ds; ++s) {
         const int yi = bs_bin(s, ps, k.mid);
         if (yi >= n || yi < 0) continue;
