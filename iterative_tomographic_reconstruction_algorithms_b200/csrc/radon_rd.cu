@@ -7,21 +7,24 @@
 // [-nh, nh]^2 at p1 and leaves at p2 (:133-179).  The walk starts in pixel
 // (round(p1x), round(p1y)) with alpha = 0 (the reference's `alpha` is
 // uninitialised; its -O3 build behaves as 0), computes the next x and y
-// crossing parameters in double precision, rounds them to float, steps across
-// the smaller (both when equal), and credits (alpha - alpha_old) * |p2 - p1| / 5
+// crossing parameters as double quotients rounded to float, steps across the
+// smaller (both when equal), and credits (alpha - alpha_old) * |p2 - p1| / 5
 // to the pixel it steps INTO (x index -> image row) if that pixel has row and
 // column in [1, n-1]; it stops after the first step with alpha > 1.
 //
-// Forward: one thread per (bin, angle) replays its five walks exactly.
-// Adjoint: one thread per pixel.  With X(a), Y(b) the a-th x and b-th y
-// crossing of a walk, the walk visits the state with A x-steps and B y-steps
-// iff X(A-1) < Y(B) and Y(B-1) < X(A); it enters it at max(X(A-1), Y(B-1)),
-// coming from the state entered at the previous crossing, and credits it iff
-// that previous alpha is <= 1.  That closed form is evaluated for the few
-// sub-rays whose line crosses the pixel, giving the exact transpose of the
-// forward without atomics.
+// Both directions run the same walks (rd_walk), one thread per (bin, angle,
+// slice) replaying its bin's five sub-rays:
+//   forward  gathers 0.2 l x[pixel] into the bin, in walk order;
+//   adjoint  scatters 0.2 l y[bin] into a 64-bit fixed-point image with
+//            integer atomics (exact, order-independent sums: deterministic),
+//            rounded to float once, through the solver epilogue, at the end.
+// The walk's arithmetic is float only: the crossing parameters reproduce the
+// reference's double quotients exactly (rd_alpha_ff), with a double division
+// only for quotients within 2^-38 of a float rounding boundary.
+#include <algorithm>
 #include <cmath>
 
+#include "fixed_sum.cuh"
 #include "tomo_internal.cuh"
 
 namespace tomo {
@@ -29,21 +32,32 @@ namespace {
 
 constexpr double kPi = 3.141592653589793;
 
-struct SubRay {
-  float p1x, p1y, ex, ey, incr;
-  int ii0, jj0, dx, dy;
-};
-
-// Sub-ray offset (radon_rd.c:125-130), i/6 compiled as fma(i, 1/6, -nh) in double.
-__device__ __forceinline__ float rd_offset(int i, int n, int nh, bool lt, bool gt) {
-  float t = (float)fabs(__fma_rn((double)i, 1.0 / 6.0, -(double)nh));
+// Sub-ray offset |i/6 - nh| (radon_rd.c:125-126) read from a table made on the
+// host in the reference's double arithmetic, with the signs of :127-130.
+__device__ __forceinline__ float rd_offset_tab(const float *__restrict__ toff, int i, int n, bool lt, bool gt) {
+  float t = __ldg(toff + i);
   if (i >= 3 * n && lt) t = -t;
   if (i < 3 * n && gt) t = -t;
   return t;
 }
 
-// Entry/exit points (radon_rd.c:133-179) in the compiled order (K + t) * (1/c).
-__device__ __forceinline__ SubRay rd_subray(float t, const RdAngle &g, int nh) {
+// (int)roundf(x) (halves away from zero) for |x| < 2^22: floor(|x| + 0.5) is
+// the floor of the round-down sum (the integer below is a float), and a
+// round-down add of 1.5 * 2^23 puts that floor in the low mantissa bits.
+__device__ __forceinline__ int rd_round_i(float x) {
+  const float f = __fadd_rd(__fadd_rd(fabsf(x), 0.5f), 12582912.0f);
+  const int k = __float_as_int(f) - 0x4B400000;
+  return x < 0.0f ? -k : k;
+}
+
+// Entry point, extents and start pixel of a sub-ray (rd_subray without the
+// length, which only the credited visits need).
+struct RdGeom {
+  float p1x, p1y, ex, ey;
+  int ii0, jj0, dx, dy;
+};
+
+__device__ __forceinline__ RdGeom rd_geom(float t, const RdAngle &g, int nh) {
   const float fnh = (float)nh;
   float p1x, p1y, p2x, p2y;
   if (g.lt) {
@@ -57,47 +71,90 @@ __device__ __forceinline__ SubRay rd_subray(float t, const RdAngle &g, int nh) {
     if (y1 >= -fnh && y1 <= fnh) { p1x = fnh; p1y = y1; } else { p1x = x1; p1y = -fnh; }
     if (y2 >= -fnh && y2 <= fnh) { p2x = -fnh; p2y = y2; } else { p2x = x2; p2y = fnh; }
   }
-  SubRay r;
+  RdGeom r;
   r.p1x = p1x;
   r.p1y = p1y;
   r.ex = __fsub_rn(p2x, p1x);
   r.ey = __fsub_rn(p2y, p1y);
-  r.incr = __fsqrt_rn(__fmaf_rn(r.ex, r.ex, __fmul_rn(r.ey, r.ey)));
-  r.ii0 = (int)roundf(p1x);
-  r.jj0 = (int)roundf(p1y);
+  r.ii0 = rd_round_i(p1x);
+  r.jj0 = rd_round_i(p1y);
   r.dx = p2x > p1x ? 1 : -1;
   r.dy = p2y > p1y ? 1 : -1;
   return r;
 }
 
-// Numerator of the crossing out of column/row state `idx`: (idx + d/2) - p,
-// exact in double.
-__device__ __forceinline__ double rd_num(int idx, int d, float p) {
-  return __dsub_rn(__dadd_rn((double)idx, 0.5 * d), (double)p);
+// alpha of the crossing at the half-integer coordinate a, for a sub-ray that
+// enters at p with extent e, r = RN(1/e): the float of the correctly rounded
+// double quotient ((double)a - p) / e that the reference computes
+// (radon_rd.c:41-42), in float arithmetic.
+//
+// a - p = h + l exactly (Knuth's TwoSum).  q1 = RN(h r); the remainder
+// h + l - q1 e (one FMA, then + l) times r gives q2, and q1 + q2 is within
+// 2^-44 |x| of the exact quotient x (r and q1 are within 2^-23 of exact, the
+// remainder is 2^-23 |h| small).  s = RN(q1 + q2), t = q1 + q2 - s exactly
+// (Fast2Sum, |q2| << |q1|).  When |t| plus 2^-38 |s| is below half an ulp of s
+// and s is not a power of two (whose rounding interval below is half as
+// wide), x rounds to s, and so does the double nearest x, which lies within
+// 2^-53 |x| of it and so on the same side of every float midpoint.  Otherwise
+// (x within 2^-38 of a midpoint, s zero, tiny, infinite or NaN) divide in
+// double.
+__device__ __forceinline__ float rd_alpha_ff(float a, float p, float e, float r) {
+  const float h = __fsub_rn(a, p);
+  const float bb = __fsub_rn(h, a);
+  const float l = __fadd_rn(__fsub_rn(a, __fsub_rn(h, bb)), __fsub_rn(-p, bb));
+  const float q1 = __fmul_rn(h, r);
+  const float rho = __fadd_rn(__fmaf_rn(-q1, e, h), l);
+  const float q2 = __fmul_rn(rho, r);
+  const float s = __fadd_rn(q1, q2);
+  const float t = __fsub_rn(q2, __fsub_rn(s, q1));
+  const unsigned sb = __float_as_uint(s) & 0x7fffffffu;
+  const float hu = __uint_as_float((sb & 0x7f800000u) - (24u << 23));  // 2^(exponent of s - 24)
+  if (sb >= (40u << 23) && sb < 0x7f800000u && (sb & 0x007fffffu) != 0u &&
+      __fmaf_rn(fabsf(s), 0x1p-38f, fabsf(t)) < hu)
+    return s;
+  return __double2float_rn(__ddiv_rn(__dadd_rn((double)h, (double)l), (double)e));
 }
 
-// alpha = the float of the double quotient num / e, as the reference computes
-// it (one double division, rounded to float).  The product num * re, re the
-// double reciprocal of e, is within 2^-51 (relative) of the correctly rounded
-// quotient Q; if it rounds to the same float after moving it down and up by
-// 2^-49 (relative), that float is Q's.  Otherwise (Q within a hair of a
-// float rounding boundary, e == 0, overflow) the division is done.
-__device__ __forceinline__ float rd_alpha_q(double num, float e, double re) {
-  const double q = __dmul_rn(num, re);
-  const double m = fabs(q) * 0x1p-49;
-  const float lo = __double2float_rn(__dsub_rn(q, m)), hi = __double2float_rn(__dadd_rn(q, m));
-  if (lo == hi) return lo;
-  return __double2float_rn(__ddiv_rn(num, (double)e));
-}
-
-// alpha of the crossing out of column/row state `idx`
-__device__ __forceinline__ float rd_alpha(int idx, int d, float p, float e, double re) {
-  return rd_alpha_q(rd_num(idx, d, p), e, re);
+// One sub-ray's walk (radon_rd.c:39-70); visit(pi, pj, l) for every credited
+// step, (pi, pj) the image row and column, l the length credited.
+template <class Visit>
+__device__ __forceinline__ void rd_walk(const RdGeom &s, int n, int nh, Visit visit) {
+  const float incr = __fsqrt_rn(__fmaf_rn(s.ex, s.ex, __fmul_rn(s.ey, s.ey)));
+  const float hx = s.dx > 0 ? 0.5f : -0.5f, hy = s.dy > 0 ? 0.5f : -0.5f;
+  const float fdx = hx + hx, fdy = hy + hy;
+  const float rx = __frcp_rn(s.ex), ry = __frcp_rn(s.ey);
+  int ii = s.ii0, jj = s.jj0;
+  // coordinates of the next x and y crossings, stepped exactly by +-1
+  float cx = __fadd_rn((float)s.ii0, hx), cy = __fadd_rn((float)s.jj0, hy);
+  float ax = rd_alpha_ff(cx, s.p1x, s.ex, rx), ay = rd_alpha_ff(cy, s.p1y, s.ey, ry);
+  float alpha = 0.0f, alpha_old = 0.0f;
+  const int guard = 4 * n + 16;  // a walk crosses at most 2n + 2 lines
+  for (int it = 0; alpha <= 1.0f && it < guard; ++it) {
+    // x step if ax < ay, y step if ax > ay, both if equal (radon_rd.c:45-58);
+    // a NaN crossing would never advance the reference: stop.  Written
+    // without branches on the step kind, so the lanes of a warp stay together:
+    // one new crossing parameter (two on a diagonal step).
+    const bool sx = ax <= ay, sy = ay <= ax;
+    if (!(sx || sy)) break;
+    alpha = sx ? ax : ay;
+    ii += sx ? s.dx : 0;
+    jj += sy ? s.dy : 0;
+    cx = sx ? __fadd_rn(cx, fdx) : cx;
+    cy = sy ? __fadd_rn(cy, fdy) : cy;
+    const float a1 = rd_alpha_ff(sx ? cx : cy, sx ? s.p1x : s.p1y, sx ? s.ex : s.ey, sx ? rx : ry);
+    ax = sx ? a1 : ax;
+    ay = sx ? ay : a1;
+    if (sx && sy) ay = rd_alpha_ff(cy, s.p1y, s.ey, ry);
+    const float l = __fmul_rn(__fsub_rn(alpha, alpha_old), incr);
+    const int pi = ii + nh, pj = jj + nh;
+    if (pi > 0 && pi < n && pj > 0 && pj < n) visit(pi, pj, l);
+    alpha_old = alpha;
+  }
 }
 
 __global__ void __launch_bounds__(128) rd_forward_kernel(
     const float *__restrict__ img, float *__restrict__ sino, const RdAngle *__restrict__ tab,
-    int n, int nh, int na, FwdEpi ep) {
+    const float *__restrict__ toff, int n, int nh, int na, FwdEpi ep) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   const int v = blockIdx.y;
   const size_t z = blockIdx.z;
@@ -113,138 +170,81 @@ __global__ void __launch_bounds__(128) rd_forward_kernel(
   } else if (g.mode == 2) {  // |c| < 1e-7: bin i <- row i (:108-117)
     for (int j = 0; j < n; ++j) acc += __ldg(I + (size_t)b * n + j);
   } else {
-    const int guard = 4 * n + 16;
     for (int r = 1; r <= 5; ++r) {
-      const int i = 6 * b + r;
-      const SubRay s = rd_subray(rd_offset(i, n, nh, g.lt, g.gt), g, nh);
-      int ii = s.ii0, jj = s.jj0;
-      float alpha = 0.0f, alpha_old = 0.0f;
-      const double rex = __drcp_rn((double)s.ex), rey = __drcp_rn((double)s.ey);
-      const double ddx = (double)s.dx, ddy = (double)s.dy;
-      // numerators of the next crossings, stepped exactly by +-1
-      double nx = rd_num(ii, s.dx, s.p1x), ny = rd_num(jj, s.dy, s.p1y);
-      float ax = rd_alpha_q(nx, s.ex, rex), ay = rd_alpha_q(ny, s.ey, rey);
-      for (int it = 0; alpha <= 1.0f && it < guard; ++it) {
-        if (ax < ay) {
-          alpha = ax;
-          ii += s.dx;
-          nx = __dadd_rn(nx, ddx);
-          ax = rd_alpha_q(nx, s.ex, rex);
-        } else if (ax > ay) {
-          alpha = ay;
-          jj += s.dy;
-          ny = __dadd_rn(ny, ddy);
-          ay = rd_alpha_q(ny, s.ey, rey);
-        } else if (ax == ay) {
-          alpha = ay;
-          ii += s.dx;
-          jj += s.dy;
-          nx = __dadd_rn(nx, ddx);
-          ny = __dadd_rn(ny, ddy);
-          ax = rd_alpha_q(nx, s.ex, rex);
-          ay = rd_alpha_q(ny, s.ey, rey);
-        } else {
-          break;  // NaN crossing: the reference would never advance
-        }
-        const float l = __fmul_rn(__fsub_rn(alpha, alpha_old), s.incr);
-        const int pi = ii + nh, pj = jj + nh;
-        if (pi > 0 && pi < n && pj > 0 && pj < n)
-          acc = fmaf(0.2f * l, __ldg(I + (size_t)pi * n + pj), acc);
-        alpha_old = alpha;
-      }
+      const RdGeom s = rd_geom(rd_offset_tab(toff, 6 * b + r, n, g.lt, g.gt), g, nh);
+      rd_walk(s, n, nh, [&](int pi, int pj, float l) {
+        acc = fmaf(0.2f * l, __ldg(I + (size_t)pi * n + pj), acc);
+      });
     }
   }
   fwd_store(ep, acc, live, z * (size_t)na * n + (size_t)v * n + (live ? b : 0), sino);
 }
 
-constexpr int kRdChunk = 256;
+// Fixed-point scale of slice z's adjoint: per angle a pixel receives at most
+// 11 credits 0.2 l |y| with l <= sqrt(2) (the segment in one pixel), below
+// 4 max|y|.
+__device__ __forceinline__ FixedScale rd_adj_scale(const unsigned *smax, int na) {
+  return fixed_scale(4.0 * (double)na * (double)__uint_as_float(*smax));
+}
 
-__global__ void __launch_bounds__(128) rd_adjoint_kernel(
-    const float *__restrict__ sino, float *__restrict__ img, const RdAngle *__restrict__ tab,
-    int n, int nh, int na, AdjEpi ep) {
-  __shared__ RdAngle stab[kRdChunk];
-  const int J = blockIdx.x * blockDim.x + threadIdx.x;  // column (walk y index jj + nh)
-  const int I = blockIdx.y * blockDim.y + threadIdx.y;  // row    (walk x index ii + nh)
+// Adjoint scatter: slice blockIdx.z of the chunk, accf its fixed-point image.
+__global__ void __launch_bounds__(128) rd_scatter_kernel(
+    const float *__restrict__ sino, unsigned long long *__restrict__ accf, const RdAngle *__restrict__ tab,
+    const float *__restrict__ toff, int n, int nh, int na, const unsigned *__restrict__ smax) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  const int v = blockIdx.y;
   const size_t z = blockIdx.z;
-  const bool live = I < n && J < n;
-  const float *S = sino + z * (size_t)na * n;
-  const int tid = threadIdx.y * blockDim.x + threadIdx.x, nthr = blockDim.x * blockDim.y;
-  const int iiP = I - nh, jjP = J - nh;
-  const bool interior = I > 0 && J > 0;
-  const float NEG = -INFINITY;
-  float acc = 0.0f;
-  for (int v0 = 0; v0 < na; v0 += kRdChunk) {
-    const int cnt = min(kRdChunk, na - v0);
-    __syncthreads();
-    for (int t = tid; t < cnt; t += nthr) stab[t] = tab[v0 + t];
-    __syncthreads();
-    if (!live) continue;
-    for (int u = 0; u < cnt; ++u) {
-      const RdAngle g = stab[u];
-      const float *row = S + (size_t)(v0 + u) * n;
-      if (g.mode == 1) {
-        if (J >= 1) acc += __ldg(row + n - 1 - J);
-        continue;
-      }
-      if (g.mode == 2) {
-        acc += __ldg(row + I);
-        continue;
-      }
-      if (!interior) continue;
-      // offset of the line through the pixel centre: y c - x s = t (lt) or x s - y c = t
-      const float tP = g.lt ? (float)jjP * g.c - (float)iiP * g.s : (float)iiP * g.s - (float)jjP * g.c;
-      const float half = 0.5f * (fabsf(g.c) + fabsf(g.s)) + 0.05f;
-      // sub-ray index i from t: lt: t = nh - i/6; gt: t = i/6 - nh (even n)
-      float ia, ib;
-      if (g.lt) { ia = 6.0f * ((float)nh - (tP + half)); ib = 6.0f * ((float)nh - (tP - half)); }
-      else      { ia = 6.0f * ((tP - half) + (float)nh); ib = 6.0f * ((tP + half) + (float)nh); }
-      int i0 = max((int)floorf(ia) - 1, 1), i1 = min((int)ceilf(ib) + 1, 6 * n - 1);
-      // odd n: sub-rays with i in [6 nh, 3n) carry the mirrored offset (radon_rd.c:127-130)
-      const bool odd = (n & 1) != 0;
-      const int extra0 = 6 * nh, extra1 = 3 * n - 1;
-      for (int pass = 0; pass < (odd ? 2 : 1); ++pass) {
-        const int a0 = pass == 0 ? i0 : extra0, a1 = pass == 0 ? i1 : extra1;
-        for (int i = a0; i <= a1; ++i) {
-          if (i % 6 == 0) continue;
-          if (pass == 1 && i >= i0 && i <= i1) continue;
-          const SubRay s = rd_subray(rd_offset(i, n, nh, g.lt, g.gt), g, nh);
-          const int A = (iiP - s.ii0) * s.dx, B = (jjP - s.jj0) * s.dy;
-          if (A < 0 || B < 0 || (A == 0 && B == 0)) continue;
-          const double rex = __drcp_rn((double)s.ex), rey = __drcp_rn((double)s.ey);
-          const float XA = rd_alpha(s.ii0 + A * s.dx, s.dx, s.p1x, s.ex, rex);
-          const float YB = rd_alpha(s.jj0 + B * s.dy, s.dy, s.p1y, s.ey, rey);
-          const float XA1 = A >= 1 ? rd_alpha(s.ii0 + (A - 1) * s.dx, s.dx, s.p1x, s.ex, rex) : NEG;
-          const float YB1 = B >= 1 ? rd_alpha(s.jj0 + (B - 1) * s.dy, s.dy, s.p1y, s.ey, rey) : NEG;
-          if (!(XA1 < YB && YB1 < XA)) continue;  // state (A, B) never visited
-          float ain, aprev;
-          if (XA1 > YB1) {  // entered by an x step from (A-1, B)
-            ain = XA1;
-            const float XA2 = A >= 2 ? rd_alpha(s.ii0 + (A - 2) * s.dx, s.dx, s.p1x, s.ex, rex) : 0.0f;
-            aprev = fmaxf(XA2, B >= 1 ? YB1 : 0.0f);
-          } else if (YB1 > XA1) {  // y step from (A, B-1)
-            ain = YB1;
-            const float YB2 = B >= 2 ? rd_alpha(s.jj0 + (B - 2) * s.dy, s.dy, s.p1y, s.ey, rey) : 0.0f;
-            aprev = fmaxf(A >= 1 ? XA1 : 0.0f, YB2);
-          } else {  // diagonal step from (A-1, B-1)
-            ain = XA1;
-            const float XA2 = A >= 2 ? rd_alpha(s.ii0 + (A - 2) * s.dx, s.dx, s.p1x, s.ex, rex) : 0.0f;
-            const float YB2 = B >= 2 ? rd_alpha(s.jj0 + (B - 2) * s.dy, s.dy, s.p1y, s.ey, rey) : 0.0f;
-            aprev = fmaxf(XA2, YB2);
-          }
-          if (!(aprev <= 1.0f)) continue;  // the walk had already stopped
-          const float l = __fmul_rn(__fsub_rn(ain, aprev), s.incr);
-          acc = fmaf(0.2f * l, __ldg(row + i / 6), acc);
-        }
-      }
+  if (b >= n) return;
+  const float y = __ldg(sino + (z * na + v) * (size_t)n + b);
+  if (y == 0.0f) return;
+  const RdAngle g = tab[v];
+  const FixedScale fs = rd_adj_scale(smax + z, na);
+  unsigned long long *F = accf + z * (size_t)n * n;
+  if (g.mode == 1) {  // column n-1-b, every row (transpose of radon_rd.c:96-105)
+    const int i = n - 1 - b;
+    if (i >= 1) {
+      const unsigned long long q = fixed_of(y, fs);
+      for (int j = 0; j < n; ++j) atomicAdd(F + (size_t)j * n + i, q);
     }
+    return;
   }
-  adj_store(ep, acc, live, z * (size_t)n * n + (size_t)(live ? I : 0) * n + (live ? J : 0), img);
+  if (g.mode == 2) {  // row b, every column (:108-117)
+    const unsigned long long q = fixed_of(y, fs);
+    for (int j = 0; j < n; ++j) atomicAdd(F + (size_t)b * n + j, q);
+    return;
+  }
+  for (int r = 1; r <= 5; ++r) {
+    const RdGeom s = rd_geom(rd_offset_tab(toff, 6 * b + r, n, g.lt, g.gt), g, nh);
+    rd_walk(s, n, nh, [&](int pi, int pj, float l) {
+      atomicAdd(F + (size_t)pi * n + pj, fixed_of(__fmul_rn(0.2f * l, y), fs));
+    });
+  }
+}
+
+// Fixed-point image -> float through the adjoint epilogue; pixel q of the
+// chunk is pixel p0 + q of the plan's images.
+__global__ void rd_finalize_kernel(const unsigned long long *__restrict__ accf, float *__restrict__ img,
+                                   size_t count, size_t per_slice, size_t p0, int na,
+                                   const unsigned *__restrict__ smax, AdjEpi ep) {
+  const size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  const bool live = q < count;
+  float val = 0.0f;
+  if (live) val = fixed_to_float(accf[q], rd_adj_scale(smax + q / per_slice, na));
+  adj_store(ep, val, live, p0 + (live ? q : 0), img);
+}
+
+// slices per adjoint chunk: fixed-point images of at most 512 MiB, and no more
+// than a grid dimension holds
+int rd_chunk(const Plan &p) {
+  const size_t per = (size_t)8 * p.g.n * p.g.n;
+  const size_t cap = std::min<size_t>(((size_t)512 << 20) / per, 65535);
+  return (int)std::max<size_t>(1, std::min<size_t>((size_t)p.g.nz, cap));
 }
 
 }  // namespace
 
 int rd_setup(Plan &p) {
-  const int na = p.g.na, nh = p.nh;
+  const int na = p.g.na, nh = p.nh, n = p.g.n;
   std::vector<RdAngle> tab(na);
   const float fnh = (float)nh;
   for (int v = 0; v < na; ++v) {
@@ -265,23 +265,45 @@ int rd_setup(Plan &p) {
     a.mnc = -fnh * c;
     tab[v] = a;
   }
+  // |i/6 - nh| per sub-ray index, i/6 compiled as fma(i, 1/6, -nh) in double
+  std::vector<float> toff((size_t)6 * n);
+  for (int i = 0; i < 6 * n; ++i) toff[i] = (float)std::fabs(std::fma((double)i, 1.0 / 6.0, -(double)nh));
   TOMO_CUDA(cudaMalloc(&p.d_angles, sizeof(RdAngle) * (size_t)na));
   TOMO_CUDA(cudaMemcpy(p.d_angles, tab.data(), sizeof(RdAngle) * (size_t)na, cudaMemcpyHostToDevice));
+  TOMO_CUDA(cudaMalloc(&p.d_aux, sizeof(float) * toff.size()));
+  TOMO_CUDA(cudaMemcpy(p.d_aux, toff.data(), sizeof(float) * toff.size(), cudaMemcpyHostToDevice));
+  // adjoint scratch: a chunk of fixed-point images, then max |y| per slice
+  p.scratch_bytes = (size_t)8 * rd_chunk(p) * n * n + sizeof(unsigned) * (size_t)p.g.nz;
+  TOMO_CUDA(cudaMalloc(&p.d_scratch, p.scratch_bytes));
   return TOMO_OK;
 }
 
 int rd_forward(Plan &p, const float *d_img, float *d_sino, cudaStream_t s, const FwdEpi &ep) {
   const int n = p.g.n, na = p.g.na, nz = p.g.nz;
   dim3 fb(128), fg((n + 127) / 128, na, nz);
-  rd_forward_kernel<<<fg, fb, 0, s>>>(d_img, d_sino, (const RdAngle *)p.d_angles, n, p.nh, na, ep);
+  rd_forward_kernel<<<fg, fb, 0, s>>>(d_img, d_sino, (const RdAngle *)p.d_angles, (const float *)p.d_aux,
+                                      n, p.nh, na, ep);
   TOMO_CUDA(cudaGetLastError());
   return TOMO_OK;
 }
 
 int rd_adjoint(Plan &p, const float *d_sino, float *d_img, cudaStream_t s, const AdjEpi &ep) {
-  const int n = p.g.n, na = p.g.na, nz = p.g.nz;
-  dim3 ab(32, 4), ag((n + 31) / 32, (n + 3) / 4, nz);
-  rd_adjoint_kernel<<<ag, ab, 0, s>>>(d_sino, d_img, (const RdAngle *)p.d_angles, n, p.nh, na, ep);
+  const int n = p.g.n, na = p.g.na, nz = p.g.nz, chunk = rd_chunk(p);
+  const size_t per_img = (size_t)n * n, per_sino = (size_t)na * n;
+  unsigned long long *accf = reinterpret_cast<unsigned long long *>(p.d_scratch);
+  unsigned *smax = reinterpret_cast<unsigned *>(accf + (size_t)chunk * per_img);
+  TOMO_CUDA(cudaMemsetAsync(smax, 0, sizeof(unsigned) * (size_t)nz, s));
+  for (int z0 = 0; z0 < nz; z0 += chunk) {
+    const int zc = std::min(chunk, nz - z0);
+    fixed_absmax_kernel<<<dim3(64, zc), 256, 0, s>>>(d_sino + (size_t)z0 * per_sino, per_sino, smax + z0);
+    TOMO_CUDA(cudaMemsetAsync(accf, 0, sizeof(unsigned long long) * zc * per_img, s));
+    rd_scatter_kernel<<<dim3((n + 127) / 128, na, zc), 128, 0, s>>>(
+        d_sino + (size_t)z0 * per_sino, accf, (const RdAngle *)p.d_angles, (const float *)p.d_aux, n, p.nh, na,
+        smax + z0);
+    const size_t count = (size_t)zc * per_img;
+    rd_finalize_kernel<<<(unsigned)((count + 255) / 256), 256, 0, s>>>(accf, d_img, count, per_img,
+                                                                         (size_t)z0 * per_img, na, smax + z0, ep);
+  }
   TOMO_CUDA(cudaGetLastError());
   return TOMO_OK;
 }

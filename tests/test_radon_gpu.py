@@ -5,7 +5,7 @@ Bars (written in each test):
   * vs the reference's own outputs (tests/golden): relative L2 <= 1e-5;
   * vs the FP64 oracle on the same inputs: relative L2 <= 1e-5;
   * adjoint dot test |<Ax,y> - <x,A^T y>| / (||Ax|| ||y||) <= 1e-5 (FP64 dots);
-  * bit-identical results on repeated runs (no atomics on any path);
+  * bit-identical results on repeated runs (no floating-point atomics on any path);
   * batched slices == slice-by-slice; device path == host path.
 """
 from __future__ import annotations
