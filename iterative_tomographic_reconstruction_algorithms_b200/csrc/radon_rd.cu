@@ -18,6 +18,11 @@
 //   adjoint  scatters 0.2 l y[bin] into a 64-bit fixed-point image with
 //            integer atomics (exact, order-independent sums: deterministic),
 //            rounded to float once, through the solver epilogue, at the end.
+// The lanes of a warp are neighbouring bins, so at each step they sit side by
+// side across the ray.  For angles whose rays run along image columns
+// (|s| > |c|) that is down a column: those angles read a transposed copy of
+// the image (forward) and scatter into a transposed fixed-point image
+// (adjoint), so neighbouring lanes touch neighbouring words.
 // The walk's arithmetic is float only: the crossing parameters reproduce the
 // reference's double quotients exactly (rd_alpha_ff), with a double division
 // only for quotients within 2^-38 of a float rounding boundary.
@@ -91,13 +96,18 @@ __device__ __forceinline__ RdGeom rd_geom(float t, const RdAngle &g, int nh) {
 // a - p = h + l exactly (Knuth's TwoSum).  q1 = RN(h r); the remainder
 // h + l - q1 e (one FMA, then + l) times r gives q2, and q1 + q2 is within
 // 2^-44 |x| of the exact quotient x (r and q1 are within 2^-23 of exact, the
-// remainder is 2^-23 |h| small).  s = RN(q1 + q2), t = q1 + q2 - s exactly
-// (Fast2Sum, |q2| << |q1|).  When |t| plus 2^-38 |s| is below half an ulp of s
-// and s is not a power of two (whose rounding interval below is half as
-// wide), x rounds to s, and so does the double nearest x, which lies within
-// 2^-53 |x| of it and so on the same side of every float midpoint.  Otherwise
-// (x within 2^-38 of a midpoint, s zero, tiny, infinite or NaN) divide in
-// double.
+// remainder is 2^-23 |h| small).  With d = 2^-38 |q1|, RN(q1 + RN(q2 - d))
+// and RN(q1 + RN(q2 + d)) round points below and above every value within
+// 2^-44 |x| of q1 + q2 (the inner roundings move them by 2^-47 at most).
+// Rounding to nearest is monotone, so when both give the same float s, x and
+// the double nearest x (2^-53 |x| from it) round to s too.  Otherwise (x within
+// about 2^-38 of a float rounding boundary, or e zero) divide in double.
+// The double division, out of line: rarely taken, and its double registers
+// stay out of the walk loops.
+__device__ __noinline__ float rd_alpha_div(float h, float l, float e) {
+  return __double2float_rn(__ddiv_rn(__dadd_rn((double)h, (double)l), (double)e));
+}
+
 __device__ __forceinline__ float rd_alpha_ff(float a, float p, float e, float r) {
   const float h = __fsub_rn(a, p);
   const float bb = __fsub_rn(h, a);
@@ -105,18 +115,12 @@ __device__ __forceinline__ float rd_alpha_ff(float a, float p, float e, float r)
   const float q1 = __fmul_rn(h, r);
   const float rho = __fadd_rn(__fmaf_rn(-q1, e, h), l);
   const float q2 = __fmul_rn(rho, r);
-  const float s = __fadd_rn(q1, q2);
-  const float t = __fsub_rn(q2, __fsub_rn(s, q1));
-  const unsigned sb = __float_as_uint(s) & 0x7fffffffu;
-  const float hu = __uint_as_float((sb & 0x7f800000u) - (24u << 23));  // 2^(exponent of s - 24)
-  if (sb >= (40u << 23) && sb < 0x7f800000u && (sb & 0x007fffffu) != 0u &&
-      __fmaf_rn(fabsf(s), 0x1p-38f, fabsf(t)) < hu)
-    return s;
-  return __double2float_rn(__ddiv_rn(__dadd_rn((double)h, (double)l), (double)e));
+  const float d = __fmul_rn(fabsf(q1), 0x1p-38f);
+  const float lo = __fadd_rn(q1, __fsub_rn(q2, d)), hi = __fadd_rn(q1, __fadd_rn(q2, d));
+  if (lo == hi) return lo;
+  return rd_alpha_div(h, l, e);
 }
 
-// One sub-ray's walk (radon_rd.c:39-70); visit(pi, pj, l) for every credited
-// step, (pi, pj) the image row and column, l the length credited.
 template <class Visit>
 __device__ __forceinline__ void rd_walk(const RdGeom &s, int n, int nh, Visit visit) {
   const float incr = __fsqrt_rn(__fmaf_rn(s.ex, s.ex, __fmul_rn(s.ey, s.ey)));
@@ -147,37 +151,60 @@ __device__ __forceinline__ void rd_walk(const RdGeom &s, int n, int nh, Visit vi
     if (sx && sy) ay = rd_alpha_ff(cy, s.p1y, s.ey, ry);
     const float l = __fmul_rn(__fsub_rn(alpha, alpha_old), incr);
     const int pi = ii + nh, pj = jj + nh;
-    if (pi > 0 && pi < n && pj > 0 && pj < n) visit(pi, pj, l);
+    if ((unsigned)(pi - 1) < (unsigned)(n - 1) && (unsigned)(pj - 1) < (unsigned)(n - 1)) visit(pi, pj, l);
     alpha_old = alpha;
   }
 }
 
+__global__ void rd_transpose_kernel(const float *__restrict__ in, float *__restrict__ out, int n) {
+  __shared__ float tile[32][33];
+  const size_t stride = (size_t)n * n;
+  const float *src = in + (size_t)blockIdx.z * stride;
+  float *dst = out + (size_t)blockIdx.z * stride;
+  const int x = blockIdx.x * 32 + threadIdx.x, y0 = blockIdx.y * 32;
+  for (int dy = threadIdx.y; dy < 32; dy += blockDim.y)
+    if (x < n && y0 + dy < n) tile[dy][threadIdx.x] = src[(size_t)(y0 + dy) * n + x];
+  __syncthreads();
+  const int ox = blockIdx.y * 32 + threadIdx.x;
+  for (int dy = threadIdx.y; dy < 32; dy += blockDim.y) {
+    const int oy = blockIdx.x * 32 + dy;
+    if (ox < n && oy < n) dst[(size_t)oy * n + ox] = tile[threadIdx.x][dy];
+  }
+}
+
+// Forward over slices z0 + blockIdx.z; imgT holds the chunk's slices transposed.
 __global__ void __launch_bounds__(128) rd_forward_kernel(
-    const float *__restrict__ img, float *__restrict__ sino, const RdAngle *__restrict__ tab,
-    const float *__restrict__ toff, int n, int nh, int na, FwdEpi ep) {
+    const float *__restrict__ img, const float *__restrict__ imgT, float *__restrict__ sino,
+    const RdAngle *__restrict__ tab, const float *__restrict__ toff, int n, int nh, int na, int z0, FwdEpi ep) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   const int v = blockIdx.y;
-  const size_t z = blockIdx.z;
+  const size_t z = (size_t)z0 + blockIdx.z;
   const bool live = b < n;
   const RdAngle g = tab[v];
-  const float *I = img + z * (size_t)n * n;
+  const float *I = img + z * (size_t)n * n, *IT = imgT + (size_t)blockIdx.z * n * n;
   float acc = 0.0f;
   if (!live) {
   } else if (g.mode == 1) {  // |s| < 1e-7: bin n-1-i <- column i, i >= 1 (radon_rd.c:96-105)
     const int i = n - 1 - b;
     if (i >= 1)
       for (int j = 0; j < n; ++j) acc += __ldg(I + (size_t)j * n + i);
-  } else if (g.mode == 2) {  // |c| < 1e-7: bin i <- row i (:108-117)
-    for (int j = 0; j < n; ++j) acc += __ldg(I + (size_t)b * n + j);
+  } else if (g.mode == 2) {  // |c| < 1e-7: bin i <- row i (:108-117), read down the transposed image
+    for (int j = 0; j < n; ++j) acc += __ldg(IT + (size_t)j * n + b);
   } else {
+    const bool tr = g.tr != 0;
+    const float *P = tr ? IT : I;
     for (int r = 1; r <= 5; ++r) {
       const RdGeom s = rd_geom(rd_offset_tab(toff, 6 * b + r, n, g.lt, g.gt), g, nh);
       rd_walk(s, n, nh, [&](int pi, int pj, float l) {
-        acc = fmaf(0.2f * l, __ldg(I + (size_t)pi * n + pj), acc);
+        acc = fmaf(0.2f * l, __ldg(P + (tr ? (size_t)pj * n + pi : (size_t)pi * n + pj)), acc);
       });
     }
   }
-  fwd_store(ep, acc, live, z * (size_t)na * n + (size_t)v * n + (live ? b : 0), sino);
+  // store through the epilogue; residual slot as in one launch over all slices
+  const size_t e = (z * na + v) * (size_t)n + (live ? b : 0);
+  double r2 = 0.0;
+  if (live) sino[e] = fwd_apply(ep, acc, e, r2);
+  fwd_resid_commit(ep, r2, ((z * gridDim.y + v) * gridDim.x + blockIdx.x) * (blockDim.x / 32) + threadIdx.x / 32);
 }
 
 // Fixed-point scale of slice z's adjoint: per angle a pixel receives at most
@@ -187,10 +214,12 @@ __device__ __forceinline__ FixedScale rd_adj_scale(const unsigned *smax, int na)
   return fixed_scale(4.0 * (double)na * (double)__uint_as_float(*smax));
 }
 
-// Adjoint scatter: slice blockIdx.z of the chunk, accf its fixed-point image.
+// Adjoint scatter: slice blockIdx.z of the chunk; accf its fixed-point image,
+// accT the transposed one that angles with |s| > |c| add into.
 __global__ void __launch_bounds__(128) rd_scatter_kernel(
-    const float *__restrict__ sino, unsigned long long *__restrict__ accf, const RdAngle *__restrict__ tab,
-    const float *__restrict__ toff, int n, int nh, int na, const unsigned *__restrict__ smax) {
+    const float *__restrict__ sino, unsigned long long *__restrict__ accf, unsigned long long *__restrict__ accT,
+    const RdAngle *__restrict__ tab, const float *__restrict__ toff, int n, int nh, int na,
+    const unsigned *__restrict__ smax) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   const int v = blockIdx.y;
   const size_t z = blockIdx.z;
@@ -199,7 +228,7 @@ __global__ void __launch_bounds__(128) rd_scatter_kernel(
   if (y == 0.0f) return;
   const RdAngle g = tab[v];
   const FixedScale fs = rd_adj_scale(smax + z, na);
-  unsigned long long *F = accf + z * (size_t)n * n;
+  unsigned long long *F = accf + z * (size_t)n * n, *FT = accT + z * (size_t)n * n;
   if (g.mode == 1) {  // column n-1-b, every row (transpose of radon_rd.c:96-105)
     const int i = n - 1 - b;
     if (i >= 1) {
@@ -208,35 +237,52 @@ __global__ void __launch_bounds__(128) rd_scatter_kernel(
     }
     return;
   }
-  if (g.mode == 2) {  // row b, every column (:108-117)
+  if (g.mode == 2) {  // row b, every column (:108-117), down the transposed image
     const unsigned long long q = fixed_of(y, fs);
-    for (int j = 0; j < n; ++j) atomicAdd(F + (size_t)b * n + j, q);
+    for (int j = 0; j < n; ++j) atomicAdd(FT + (size_t)j * n + b, q);
     return;
   }
+  const bool tr = g.tr != 0;
+  unsigned long long *P = tr ? FT : F;
+  // y 2^E: scaling by a power of two commutes with the rounding of the
+  // product, so each credit is fixed_of(0.2 l y) with one multiply fewer
+  const float ys = __fmul_rn(__fmul_rn(y, fs.s1), fs.s2);
   for (int r = 1; r <= 5; ++r) {
     const RdGeom s = rd_geom(rd_offset_tab(toff, 6 * b + r, n, g.lt, g.gt), g, nh);
     rd_walk(s, n, nh, [&](int pi, int pj, float l) {
-      atomicAdd(F + (size_t)pi * n + pj, fixed_of(__fmul_rn(0.2f * l, y), fs));
+      atomicAdd(P + (tr ? (size_t)pj * n + pi : (size_t)pi * n + pj),
+                (unsigned long long)__float2ll_rn(__fmul_rn(0.2f * l, ys)));
     });
   }
 }
 
-// Fixed-point image -> float through the adjoint epilogue; pixel q of the
-// chunk is pixel p0 + q of the plan's images.
-__global__ void rd_finalize_kernel(const unsigned long long *__restrict__ accf, float *__restrict__ img,
-                                   size_t count, size_t per_slice, size_t p0, int na,
-                                   const unsigned *__restrict__ smax, AdjEpi ep) {
-  const size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-  const bool live = q < count;
-  float val = 0.0f;
-  if (live) val = fixed_to_float(accf[q], rd_adj_scale(smax + q / per_slice, na));
-  adj_store(ep, val, live, p0 + (live ? q : 0), img);
+// accf + accT transposed -> float through the adjoint epilogue, a 32 x 32 tile
+// per block (blockDim 32 x 8); slice blockIdx.z of the chunk is slice z0 + it.
+__global__ void rd_finalize_kernel(const unsigned long long *__restrict__ accf,
+                                   const unsigned long long *__restrict__ accT, float *__restrict__ img, int n,
+                                   int z0, int na, const unsigned *__restrict__ smax, AdjEpi ep) {
+  __shared__ unsigned long long tile[32][33];
+  const size_t zl = blockIdx.z, per = (size_t)n * n;
+  const unsigned long long *F = accf + zl * per, *FT = accT + zl * per;
+  const int R0 = blockIdx.y * 32, C0 = blockIdx.x * 32;
+  for (int k = threadIdx.y; k < 32; k += blockDim.y)  // tile[c][r] = accT[(C0 + c) n + R0 + r]
+    if (C0 + k < n && R0 + threadIdx.x < n) tile[k][threadIdx.x] = FT[(size_t)(C0 + k) * n + R0 + threadIdx.x];
+  __syncthreads();
+  const FixedScale fs = rd_adj_scale(smax + zl, na);
+  for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+    const int R = R0 + k, C = C0 + threadIdx.x;
+    const bool live = R < n && C < n;
+    float val = 0.0f;
+    if (live) val = fixed_to_float(F[(size_t)R * n + C] + tile[threadIdx.x][k], fs);
+    adj_store(ep, val, live, ((size_t)z0 + zl) * per + (live ? (size_t)R * n + C : 0), img);
+  }
 }
 
-// slices per adjoint chunk: fixed-point images of at most 512 MiB, and no more
-// than a grid dimension holds
+// slices per chunk: the adjoint's two fixed-point images (the forward's
+// transposed image uses the same space) of at most 512 MiB, and no more than a
+// grid dimension holds
 int rd_chunk(const Plan &p) {
-  const size_t per = (size_t)8 * p.g.n * p.g.n;
+  const size_t per = (size_t)16 * p.g.n * p.g.n;
   const size_t cap = std::min<size_t>(((size_t)512 << 20) / per, 65535);
   return (int)std::max<size_t>(1, std::min<size_t>((size_t)p.g.nz, cap));
 }
@@ -257,6 +303,7 @@ int rd_setup(Plan &p) {
     a.mode = std::fabs((double)s) < 1e-7 ? 1 : (std::fabs((double)c) < 1e-7 ? 2 : 0);
     a.lt = (double)theta < kPi / 2;
     a.gt = (double)theta > kPi / 2;
+    a.tr = std::fabs((double)s) > std::fabs((double)c) ? 1 : 0;
     a.rc = 1.0f / c;
     a.rs = 1.0f / s;
     a.ns = fnh * s;
@@ -272,17 +319,23 @@ int rd_setup(Plan &p) {
   TOMO_CUDA(cudaMemcpy(p.d_angles, tab.data(), sizeof(RdAngle) * (size_t)na, cudaMemcpyHostToDevice));
   TOMO_CUDA(cudaMalloc(&p.d_aux, sizeof(float) * toff.size()));
   TOMO_CUDA(cudaMemcpy(p.d_aux, toff.data(), sizeof(float) * toff.size(), cudaMemcpyHostToDevice));
-  // adjoint scratch: a chunk of fixed-point images, then max |y| per slice
-  p.scratch_bytes = (size_t)8 * rd_chunk(p) * n * n + sizeof(unsigned) * (size_t)p.g.nz;
+  // scratch: a chunk of fixed-point images and of transposed ones (the
+  // forward's transposed images in the same space), then max |y| per slice
+  p.scratch_bytes = (size_t)16 * rd_chunk(p) * n * n + sizeof(unsigned) * (size_t)p.g.nz;
   TOMO_CUDA(cudaMalloc(&p.d_scratch, p.scratch_bytes));
   return TOMO_OK;
 }
 
 int rd_forward(Plan &p, const float *d_img, float *d_sino, cudaStream_t s, const FwdEpi &ep) {
-  const int n = p.g.n, na = p.g.na, nz = p.g.nz;
-  dim3 fb(128), fg((n + 127) / 128, na, nz);
-  rd_forward_kernel<<<fg, fb, 0, s>>>(d_img, d_sino, (const RdAngle *)p.d_angles, (const float *)p.d_aux,
-                                      n, p.nh, na, ep);
+  const int n = p.g.n, na = p.g.na, nz = p.g.nz, chunk = rd_chunk(p);
+  float *imgT = p.d_scratch;
+  for (int z0 = 0; z0 < nz; z0 += chunk) {
+    const int zc = std::min(chunk, nz - z0);
+    rd_transpose_kernel<<<dim3((n + 31) / 32, (n + 31) / 32, zc), dim3(32, 8), 0, s>>>(
+        d_img + (size_t)z0 * n * n, imgT, n);
+    rd_forward_kernel<<<dim3((n + 127) / 128, na, zc), 128, 0, s>>>(
+        d_img, imgT, d_sino, (const RdAngle *)p.d_angles, (const float *)p.d_aux, n, p.nh, na, z0, ep);
+  }
   TOMO_CUDA(cudaGetLastError());
   return TOMO_OK;
 }
@@ -291,18 +344,19 @@ int rd_adjoint(Plan &p, const float *d_sino, float *d_img, cudaStream_t s, const
   const int n = p.g.n, na = p.g.na, nz = p.g.nz, chunk = rd_chunk(p);
   const size_t per_img = (size_t)n * n, per_sino = (size_t)na * n;
   unsigned long long *accf = reinterpret_cast<unsigned long long *>(p.d_scratch);
-  unsigned *smax = reinterpret_cast<unsigned *>(accf + (size_t)chunk * per_img);
+  unsigned long long *accT = accf + (size_t)chunk * per_img;
+  unsigned *smax = reinterpret_cast<unsigned *>(accT + (size_t)chunk * per_img);
   TOMO_CUDA(cudaMemsetAsync(smax, 0, sizeof(unsigned) * (size_t)nz, s));
   for (int z0 = 0; z0 < nz; z0 += chunk) {
     const int zc = std::min(chunk, nz - z0);
     fixed_absmax_kernel<<<dim3(64, zc), 256, 0, s>>>(d_sino + (size_t)z0 * per_sino, per_sino, smax + z0);
     TOMO_CUDA(cudaMemsetAsync(accf, 0, sizeof(unsigned long long) * zc * per_img, s));
+    TOMO_CUDA(cudaMemsetAsync(accT, 0, sizeof(unsigned long long) * zc * per_img, s));
     rd_scatter_kernel<<<dim3((n + 127) / 128, na, zc), 128, 0, s>>>(
-        d_sino + (size_t)z0 * per_sino, accf, (const RdAngle *)p.d_angles, (const float *)p.d_aux, n, p.nh, na,
-        smax + z0);
-    const size_t count = (size_t)zc * per_img;
-    rd_finalize_kernel<<<(unsigned)((count + 255) / 256), 256, 0, s>>>(accf, d_img, count, per_img,
-                                                                         (size_t)z0 * per_img, na, smax + z0, ep);
+        d_sino + (size_t)z0 * per_sino, accf, accT, (const RdAngle *)p.d_angles, (const float *)p.d_aux, n, p.nh,
+        na, smax + z0);
+    rd_finalize_kernel<<<dim3((n + 31) / 32, (n + 31) / 32, zc), dim3(32, 8), 0, s>>>(
+        accf, accT, d_img, n, z0, na, smax + z0, ep);
   }
   TOMO_CUDA(cudaGetLastError());
   return TOMO_OK;

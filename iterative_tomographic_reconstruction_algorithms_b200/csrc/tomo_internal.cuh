@@ -67,6 +67,7 @@ struct RdAngle {
   float ns, nc, mns, mnc;  // nh*s, nh*c, -nh*s, -nh*c
   int mode;                // 0 general, 1 |s| < 1e-7, 2 |c| < 1e-7
   int lt, gt;              // theta < pi/2, theta > pi/2
+  int tr;                  // |s| > |c|: walks run along image columns; use the transposed image
 };
 
 struct Plan {

