@@ -40,6 +40,11 @@ def radon_golden():
 
 
 @pytest.fixture(scope="session")
+def dd_entries_golden():
+    return np.load(GOLDEN / "dd_entries_golden.npz")
+
+
+@pytest.fixture(scope="session")
 def bspline_golden():
     return np.load(GOLDEN / "bspline_golden.npz")
 
