@@ -13,6 +13,8 @@
 #include <thread>
 #include <atomic>
 #include <algorithm>
+#include <condition_variable>
+#include <functional>
 
 #include "tomo_internal.cuh"
 
@@ -259,36 +261,105 @@ static int ensure_host_buffers(Plan &p) {
   return TOMO_OK;
 }
 
-// Host <-> device copies through the pinned staging buffer, in chunks: several
+// Host <-> device copies through the pinned staging buffer, in 1 MiB chunks:
 // host threads copy chunks between the caller's array and the staging buffer,
 // and each chunk's DMA is queued as soon as its host copy is done (and the
 // host copy of an output chunk starts as soon as its DMA has landed), so the
-// memcpy and the transfer overlap.
-constexpr size_t kStageChunk = (size_t)4 << 20;
+// copies and the transfers overlap.  The threads are a pool kept across calls.
+constexpr size_t kStageChunk = (size_t)1 << 20;
 
-static int stage_threads(size_t bytes) {
-  const unsigned hc = std::thread::hardware_concurrency();
-  const size_t by_size = (bytes + kStageChunk - 1) / kStageChunk;
-  return (int)std::max<size_t>(1, std::min<size_t>({(size_t)8, (size_t)(hc ? hc / 2 : 1), by_size}));
-}
+// A fixed pool of host threads; run(n, f) calls f(0 .. n-1) on the pool and on
+// the calling thread and returns when every call has returned.  One run at a
+// time; a worker claims tasks only of the run it was woken for.
+class StagePool {
+ public:
+  static StagePool &get() {
+    static StagePool pool;
+    return pool;
+  }
+
+  void run(int n, const std::function<void(int)> &f) {
+    std::lock_guard<std::mutex> one(run_mu_);
+    unsigned g;
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      job_ = &f;
+      n_ = n;
+      next_ = 0;
+      done_ = 0;
+      g = ++gen_;
+    }
+    cv_.notify_all();
+    work(g);
+    std::unique_lock<std::mutex> lk(mu_);
+    done_cv_.wait(lk, [&] { return done_ == n_; });
+    job_ = nullptr;
+  }
+
+  ~StagePool() {
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      stop_ = true;
+    }
+    cv_.notify_all();
+    for (auto &t : workers_) t.join();
+  }
+
+ private:
+  StagePool() {
+    const unsigned hc = std::thread::hardware_concurrency();
+    const int nw = std::max(0, (int)std::min(8u, std::max(1u, hc / 2)) - 1);
+    for (int i = 0; i < nw; ++i)
+      workers_.emplace_back([this] {
+        unsigned seen = 0;
+        for (;;) {
+          unsigned g;
+          {
+            std::unique_lock<std::mutex> lk(mu_);
+            cv_.wait(lk, [&] { return stop_ || gen_ != seen; });
+            if (stop_) return;
+            g = seen = gen_;
+          }
+          work(g);
+        }
+      });
+  }
+
+  void work(unsigned g) {
+    for (;;) {
+      int t;
+      const std::function<void(int)> *f;
+      {
+        std::lock_guard<std::mutex> lk(mu_);
+        if (gen_ != g || job_ == nullptr || next_ >= n_) return;
+        t = next_++;
+        f = job_;
+      }
+      (*f)(t);
+      std::lock_guard<std::mutex> lk(mu_);
+      if (++done_ == n_) done_cv_.notify_all();
+    }
+  }
+
+  std::mutex run_mu_, mu_;
+  std::condition_variable cv_, done_cv_;
+  std::vector<std::thread> workers_;
+  const std::function<void(int)> *job_ = nullptr;
+  int n_ = 0, next_ = 0, done_ = 0;
+  unsigned gen_ = 0;
+  bool stop_ = false;
+};
 
 static int stage_in(Plan &p, const void *src, void *dst, size_t bytes) {
   const size_t nch = (bytes + kStageChunk - 1) / kStageChunk;
-  const int nt = stage_threads(bytes);
   std::atomic<int> err{0};
-  auto work = [&](int t) {
-    for (size_t c = (size_t)t; c < nch; c += (size_t)nt) {
-      const size_t off = c * kStageChunk, len = std::min(kStageChunk, bytes - off);
-      std::memcpy(p.h_stage + off, (const char *)src + off, len);
-      if (cudaMemcpyAsync((char *)dst + off, p.h_stage + off, len, cudaMemcpyHostToDevice, p.host_stream) !=
-          cudaSuccess)
-        err = 1;
-    }
-  };
-  std::vector<std::thread> th;
-  for (int t = 1; t < nt; ++t) th.emplace_back(work, t);
-  work(0);
-  for (auto &x : th) x.join();
+  StagePool::get().run((int)nch, [&](int c) {
+    const size_t off = (size_t)c * kStageChunk, len = std::min(kStageChunk, bytes - off);
+    std::memcpy(p.h_stage + off, (const char *)src + off, len);
+    if (cudaMemcpyAsync((char *)dst + off, p.h_stage + off, len, cudaMemcpyHostToDevice, p.host_stream) !=
+        cudaSuccess)
+      err = 1;
+  });
   if (err) return cuda_fail(cudaGetLastError(), "staged host-to-device copy");
   return TOMO_OK;
 }
@@ -306,22 +377,15 @@ static int stage_out(Plan &p, const void *src, void *dst, size_t bytes) {
                               p.host_stream));
     TOMO_CUDA(cudaEventRecord(p.stage_events[c], p.host_stream));
   }
-  const int nt = stage_threads(bytes);
   std::atomic<int> err{0};
-  auto work = [&](int t) {
-    for (size_t c = (size_t)t; c < nch; c += (size_t)nt) {
-      const size_t off = c * kStageChunk, len = std::min(kStageChunk, bytes - off);
-      if (cudaEventSynchronize(p.stage_events[c]) != cudaSuccess) {
-        err = 1;
-        continue;
-      }
-      std::memcpy((char *)dst + off, p.h_stage + off, len);
+  StagePool::get().run((int)nch, [&](int c) {
+    const size_t off = (size_t)c * kStageChunk, len = std::min(kStageChunk, bytes - off);
+    if (cudaEventSynchronize(p.stage_events[c]) != cudaSuccess) {
+      err = 1;
+      return;
     }
-  };
-  std::vector<std::thread> th;
-  for (int t = 1; t < nt; ++t) th.emplace_back(work, t);
-  work(0);
-  for (auto &x : th) x.join();
+    std::memcpy((char *)dst + off, p.h_stage + off, len);
+  });
   if (err) return cuda_fail(cudaGetLastError(), "staged device-to-host copy");
   return TOMO_OK;
 }
