@@ -55,8 +55,8 @@ __device__ __forceinline__ int rd_round_i(float x) {
   return x < 0.0f ? -k : k;
 }
 
-// Entry point, extents and start pixel of a sub-ray (rd_subray without the
-// length, which only the credited visits need).
+// Entry point, extents, start pixel and step directions of a sub-ray at
+// offset t (radon_rd.c:133-179 and :21-36); the walk computes its length.
 struct RdGeom {
   float p1x, p1y, ex, ey;
   int ii0, jj0, dx, dy;
@@ -88,6 +88,12 @@ __device__ __forceinline__ RdGeom rd_geom(float t, const RdAngle &g, int nh) {
   return r;
 }
 
+// The double division of rd_alpha_ff, out of line: rarely taken, and its
+// double registers stay out of the walk loops.
+__device__ __noinline__ float rd_alpha_div(float h, float l, float e) {
+  return __double2float_rn(__ddiv_rn(__dadd_rn((double)h, (double)l), (double)e));
+}
+
 // alpha of the crossing at the half-integer coordinate a, for a sub-ray that
 // enters at p with extent e, r = RN(1/e): the float of the correctly rounded
 // double quotient ((double)a - p) / e that the reference computes
@@ -102,12 +108,6 @@ __device__ __forceinline__ RdGeom rd_geom(float t, const RdAngle &g, int nh) {
 // Rounding to nearest is monotone, so when both give the same float s, x and
 // the double nearest x (2^-53 |x| from it) round to s too.  Otherwise (x within
 // about 2^-38 of a float rounding boundary, or e zero) divide in double.
-// The double division, out of line: rarely taken, and its double registers
-// stay out of the walk loops.
-__device__ __noinline__ float rd_alpha_div(float h, float l, float e) {
-  return __double2float_rn(__ddiv_rn(__dadd_rn((double)h, (double)l), (double)e));
-}
-
 __device__ __forceinline__ float rd_alpha_ff(float a, float p, float e, float r) {
   const float h = __fsub_rn(a, p);
   const float bb = __fsub_rn(h, a);
@@ -121,6 +121,8 @@ __device__ __forceinline__ float rd_alpha_ff(float a, float p, float e, float r)
   return rd_alpha_div(h, l, e);
 }
 
+// One sub-ray's walk (radon_rd.c:39-70): visit(pi, pj, l) for every credited
+// step, (pi, pj) the image row and column stepped into, l the length credited.
 template <class Visit>
 __device__ __forceinline__ void rd_walk(const RdGeom &s, int n, int nh, Visit visit) {
   const float incr = __fsqrt_rn(__fmaf_rn(s.ex, s.ex, __fmul_rn(s.ey, s.ey)));
@@ -208,8 +210,9 @@ __global__ void __launch_bounds__(128) rd_forward_kernel(
 }
 
 // Fixed-point scale of slice z's adjoint: per angle a pixel receives at most
-// 11 credits 0.2 l |y| with l <= sqrt(2) (the segment in one pixel), below
-// 4 max|y|.
+// 11 credits 0.2 l |y| with l <= sqrt(2) (the segment in one pixel), or one
+// credit |y| (row and column sums), below 4 max|y|; the bound holds for each of
+// the two fixed-point images and for their sum.
 __device__ __forceinline__ FixedScale rd_adj_scale(const unsigned *smax, int na) {
   return fixed_scale(4.0 * (double)na * (double)__uint_as_float(*smax));
 }
