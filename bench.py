@@ -583,7 +583,7 @@ def main():
     h2d = img_np.nbytes + b_np.nbytes
     d2h = b_np.nbytes + g_np.nbytes
 
-    # roofline of the dominant kernel (per survey: L1/shared-memory gather bound)
+    # roofline of the dominant kernel (the projectors are bound by L1/shared-memory gathers)
     dom_ms = max(fwd_ms, adj_ms)
     dom = "adjoint" if adj_ms >= fwd_ms else "forward"
     upd_app = n * n * na

@@ -1,4 +1,4 @@
-"""CPU tests of the oracle: it must reproduce the reference before it may judge the GPU.
+"""CPU tests of the oracle: it must reproduce the reference before it may check the GPU.
 
 * against the golden fixtures (reference outputs stored in tests/golden/);
 * against the compiled reference itself on fresh random inputs and on
