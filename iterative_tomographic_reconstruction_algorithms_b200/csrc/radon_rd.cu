@@ -18,6 +18,10 @@
 //   adjoint  scatters 0.2 l y[bin] into a 64-bit fixed-point image with
 //            integer atomics (exact, order-independent sums: deterministic),
 //            rounded to float once, through the solver epilogue, at the end.
+//            Non-finite credits (inf or NaN in y, or 0 * inf) cannot be held
+//            as integers: they set per-pixel flags instead, and a flagged
+//            pixel becomes what the reference's float sum gives (+inf, -inf,
+//            or NaN when it met NaN or both infinities).
 // The lanes of a warp are neighbouring bins, so at each step they sit side by
 // side across the ray.  For angles whose rays run along image columns
 // (|s| > |c|) that is down a column: those angles read a transposed copy of
@@ -209,6 +213,47 @@ __global__ void __launch_bounds__(128) rd_forward_kernel(
   fwd_resid_commit(ep, r2, ((z * gridDim.y + v) * gridDim.x + blockIdx.x) * (blockDim.x / 32) + threadIdx.x / 32);
 }
 
+// Per slice z (blockIdx.y): out[z] = max |x| over the finite x, as float bits.
+__global__ void rd_finite_absmax_kernel(const float *__restrict__ x, size_t per_slice, unsigned *__restrict__ out) {
+  const size_t z = blockIdx.y;
+  unsigned m = 0u;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < per_slice; i += (size_t)gridDim.x * blockDim.x) {
+    const unsigned b = __float_as_uint(fabsf(__ldg(x + z * per_slice + i)));
+    if (b < 0x7f800000u) m = max(m, b);
+  }
+  for (int off = 16; off; off >>= 1) m = max(m, __shfl_down_sync(0xffffffffu, m, off));
+  if ((threadIdx.x & 31) == 0 && m) atomicMax(out + z, m);
+}
+
+// Flags of a non-finite credit c: 1 +inf, 2 -inf, 4 NaN; set in byte p of the
+// chunk's flag array (four pixels to a 32-bit word).
+constexpr unsigned kRdPosInf = 1u, kRdNegInf = 2u, kRdNaN = 4u;
+
+__device__ __forceinline__ void rd_flag(unsigned *flags, size_t p, float c) {
+  const unsigned f = c != c ? kRdNaN : (c > 0.0f ? kRdPosInf : kRdNegInf);
+  atomicOr(flags + (p >> 2), f << (8u * (unsigned)(p & 3)));
+}
+
+// The adjoint scatter of a bin whose value y is inf or NaN: the same walks
+// (and row / column sums), flags instead of sums, in the natural pixel layout.
+// Out of line: rarely taken, and kept out of the register budget of the walk.
+__device__ __noinline__ void rd_scatter_nonfinite(float y, const RdAngle *__restrict__ gp, int b, int n, int nh,
+                                                  const float *__restrict__ toff, unsigned *Fl) {
+  const RdAngle g = *gp;
+  if (g.mode == 1) {
+    const int i = n - 1 - b;
+    if (i >= 1)
+      for (int j = 0; j < n; ++j) rd_flag(Fl, (size_t)j * n + i, y);
+  } else if (g.mode == 2) {
+    for (int j = 0; j < n; ++j) rd_flag(Fl, (size_t)b * n + j, y);
+  } else {
+    for (int r = 1; r <= 5; ++r) {
+      const RdGeom s = rd_geom(rd_offset_tab(toff, 6 * b + r, n, g.lt, g.gt), g, nh);
+      rd_walk(s, n, nh, [&](int pi, int pj, float l) { rd_flag(Fl, (size_t)pi * n + pj, __fmul_rn(0.2f * l, y)); });
+    }
+  }
+}
+
 // Fixed-point scale of slice z's adjoint: per angle a pixel receives at most
 // 11 credits 0.2 l |y| with l <= sqrt(2) (the segment in one pixel), or one
 // credit |y| (row and column sums), below 4 max|y|; the bound holds for each of
@@ -221,8 +266,8 @@ __device__ __forceinline__ FixedScale rd_adj_scale(const unsigned *smax, int na)
 // accT the transposed one that angles with |s| > |c| add into.
 __global__ void __launch_bounds__(128) rd_scatter_kernel(
     const float *__restrict__ sino, unsigned long long *__restrict__ accf, unsigned long long *__restrict__ accT,
-    const RdAngle *__restrict__ tab, const float *__restrict__ toff, int n, int nh, int na,
-    const unsigned *__restrict__ smax) {
+    unsigned *__restrict__ flags, const RdAngle *__restrict__ tab, const float *__restrict__ toff, int n, int nh,
+    int na, const unsigned *__restrict__ smax) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   const int v = blockIdx.y;
   const size_t z = blockIdx.z;
@@ -230,6 +275,10 @@ __global__ void __launch_bounds__(128) rd_scatter_kernel(
   const float y = __ldg(sino + (z * na + v) * (size_t)n + b);
   if (y == 0.0f) return;
   const RdAngle g = tab[v];
+  if (!(fabsf(y) <= 3.4028235e38f)) {  // inf or NaN
+    rd_scatter_nonfinite(y, tab + v, b, n, nh, toff, flags + z * (((size_t)n * n + 3) / 4));
+    return;
+  }
   const FixedScale fs = rd_adj_scale(smax + z, na);
   unsigned long long *F = accf + z * (size_t)n * n, *FT = accT + z * (size_t)n * n;
   if (g.mode == 1) {  // column n-1-b, every row (transpose of radon_rd.c:96-105)
@@ -262,8 +311,9 @@ __global__ void __launch_bounds__(128) rd_scatter_kernel(
 // accf + accT transposed -> float through the adjoint epilogue, a 32 x 32 tile
 // per block (blockDim 32 x 8); slice blockIdx.z of the chunk is slice z0 + it.
 __global__ void rd_finalize_kernel(const unsigned long long *__restrict__ accf,
-                                   const unsigned long long *__restrict__ accT, float *__restrict__ img, int n,
-                                   int z0, int na, const unsigned *__restrict__ smax, AdjEpi ep) {
+                                   const unsigned long long *__restrict__ accT, const unsigned *__restrict__ flags,
+                                   float *__restrict__ img, int n, int z0, int na, const unsigned *__restrict__ smax,
+                                   AdjEpi ep) {
   __shared__ unsigned long long tile[32][33];
   const size_t zl = blockIdx.z, per = (size_t)n * n;
   const unsigned long long *F = accf + zl * per, *FT = accT + zl * per;
@@ -276,16 +326,24 @@ __global__ void rd_finalize_kernel(const unsigned long long *__restrict__ accf,
     const int R = R0 + k, C = C0 + threadIdx.x;
     const bool live = R < n && C < n;
     float val = 0.0f;
-    if (live) val = fixed_to_float(F[(size_t)R * n + C] + tile[threadIdx.x][k], fs);
+    if (live) {
+      const size_t p = (size_t)R * n + C;
+      const unsigned f = (flags[zl * ((per + 3) / 4) + (p >> 2)] >> (8u * (unsigned)(p & 3))) & 0xffu;
+      if (f == 0u) val = fixed_to_float(F[p] + tile[threadIdx.x][k], fs);
+      else if ((f & kRdNaN) || f == (kRdPosInf | kRdNegInf)) val = __int_as_float(0x7fffffff);
+      else val = (f & kRdPosInf) ? __int_as_float(0x7f800000) : __int_as_float(0xff800000);
+    }
     adj_store(ep, val, live, ((size_t)z0 + zl) * per + (live ? (size_t)R * n + C : 0), img);
   }
 }
 
-// slices per chunk: the adjoint's two fixed-point images (the forward's
-// transposed image uses the same space) of at most 512 MiB, and no more than a
-// grid dimension holds
+// slices per chunk: the adjoint's two fixed-point images and flag bytes (the
+// forward's transposed image uses the same space) of at most 512 MiB, and no
+// more than a grid dimension holds
+size_t rd_flag_words(const Plan &p) { return ((size_t)p.g.n * p.g.n + 3) / 4; }
+
 int rd_chunk(const Plan &p) {
-  const size_t per = (size_t)16 * p.g.n * p.g.n;
+  const size_t per = (size_t)16 * p.g.n * p.g.n + 4 * rd_flag_words(p);
   const size_t cap = std::min<size_t>(((size_t)512 << 20) / per, 65535);
   return (int)std::max<size_t>(1, std::min<size_t>((size_t)p.g.nz, cap));
 }
@@ -322,9 +380,10 @@ int rd_setup(Plan &p) {
   TOMO_CUDA(cudaMemcpy(p.d_angles, tab.data(), sizeof(RdAngle) * (size_t)na, cudaMemcpyHostToDevice));
   TOMO_CUDA(cudaMalloc(&p.d_aux, sizeof(float) * toff.size()));
   TOMO_CUDA(cudaMemcpy(p.d_aux, toff.data(), sizeof(float) * toff.size(), cudaMemcpyHostToDevice));
-  // scratch: a chunk of fixed-point images and of transposed ones (the
-  // forward's transposed images in the same space), then max |y| per slice
-  p.scratch_bytes = (size_t)16 * rd_chunk(p) * n * n + sizeof(unsigned) * (size_t)p.g.nz;
+  // scratch: a chunk of fixed-point images, of transposed ones and of flag
+  // bytes (the forward's transposed images in the same space), then max |y|
+  // per slice
+  p.scratch_bytes = ((size_t)16 * n * n + 4 * rd_flag_words(p)) * rd_chunk(p) + sizeof(unsigned) * (size_t)p.g.nz;
   TOMO_CUDA(cudaMalloc(&p.d_scratch, p.scratch_bytes));
   return TOMO_OK;
 }
@@ -348,18 +407,21 @@ int rd_adjoint(Plan &p, const float *d_sino, float *d_img, cudaStream_t s, const
   const size_t per_img = (size_t)n * n, per_sino = (size_t)na * n;
   unsigned long long *accf = reinterpret_cast<unsigned long long *>(p.d_scratch);
   unsigned long long *accT = accf + (size_t)chunk * per_img;
-  unsigned *smax = reinterpret_cast<unsigned *>(accT + (size_t)chunk * per_img);
+  const size_t fw = rd_flag_words(p);
+  unsigned *flags = reinterpret_cast<unsigned *>(accT + (size_t)chunk * per_img);
+  unsigned *smax = flags + (size_t)chunk * fw;
   TOMO_CUDA(cudaMemsetAsync(smax, 0, sizeof(unsigned) * (size_t)nz, s));
   for (int z0 = 0; z0 < nz; z0 += chunk) {
     const int zc = std::min(chunk, nz - z0);
-    fixed_absmax_kernel<<<dim3(64, zc), 256, 0, s>>>(d_sino + (size_t)z0 * per_sino, per_sino, smax + z0);
+    rd_finite_absmax_kernel<<<dim3(64, zc), 256, 0, s>>>(d_sino + (size_t)z0 * per_sino, per_sino, smax + z0);
     TOMO_CUDA(cudaMemsetAsync(accf, 0, sizeof(unsigned long long) * zc * per_img, s));
     TOMO_CUDA(cudaMemsetAsync(accT, 0, sizeof(unsigned long long) * zc * per_img, s));
+    TOMO_CUDA(cudaMemsetAsync(flags, 0, sizeof(unsigned) * zc * fw, s));
     rd_scatter_kernel<<<dim3((n + 127) / 128, na, zc), 128, 0, s>>>(
-        d_sino + (size_t)z0 * per_sino, accf, accT, (const RdAngle *)p.d_angles, (const float *)p.d_aux, n, p.nh,
-        na, smax + z0);
+        d_sino + (size_t)z0 * per_sino, accf, accT, flags, (const RdAngle *)p.d_angles, (const float *)p.d_aux, n,
+        p.nh, na, smax + z0);
     rd_finalize_kernel<<<dim3((n + 31) / 32, (n + 31) / 32, zc), dim3(32, 8), 0, s>>>(
-        accf, accT, d_img, n, z0, na, smax + z0, ep);
+        accf, accT, flags, d_img, n, z0, na, smax + z0, ep);
   }
   TOMO_CUDA(cudaGetLastError());
   return TOMO_OK;

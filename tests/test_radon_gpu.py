@@ -126,3 +126,22 @@ def test_dd_rejects_angles_outside_domain(cuda):
     from iterative_tomographic_reconstruction_algorithms_b200 import class_projectors_radon as cpr
     with pytest.raises(ValueError, match="outside"):
         cpr.projectors(32, np.array([0.0, 200.0]), oper="dd").A(np.zeros((32, 32), np.float32))
+
+
+def test_rd_adjoint_carries_non_finite_values(cuda, oracle):
+    """inf and NaN in the sinogram reach the pixels their rays credit as the
+    reference's float sums carry them: +-inf, or NaN where NaN, 0 * inf or both
+    infinities meet (the FP64 oracle accumulates the same credits)."""
+    n, na = 64, 60
+    deg = np.linspace(0, 180, na, endpoint=False)          # 0 and 90 degrees: row / column sums
+    rng = np.random.default_rng(3)
+    y = rng.standard_normal((na, n)).astype(np.float32)
+    y[5, 20], y[17, 40], y[33, 31] = np.inf, -np.inf, np.nan
+    y[0, 10], y[30, 12], y[41, 22] = np.inf, -np.inf, np.inf
+    got = _proj("rd", n, deg).At(y)
+    ref = oracle.radon("rd", 1, y, radon_angles(deg))
+    for test in (np.isnan, np.isposinf, np.isneginf):
+        assert np.array_equal(test(got), test(ref)), test.__name__
+    fin = np.isfinite(ref)
+    assert fin.sum() > n * n // 4
+    assert rel_l2(got[fin], ref[fin]) <= TOL
