@@ -594,7 +594,7 @@ def main():
                 "unit": "GB/s", "frac": achieved / peak,
                 "traffic": DRAM_BYTES_PER_LAUNCH.get(dom),
                 "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one full-size launch "
-                                  "(profiles/dd_pair_2048x1800.md)",
+                                  "(committed ncu summary of the dd pair)",
                 "peak_source": "tomo_measure_onchip_peaks (4-byte L1 loads, this run)"}
     hbm_bytes = 4.0 * (n * n + na * n)
     peaks_file = ROOT / "MEASURED_PEAKS.json"

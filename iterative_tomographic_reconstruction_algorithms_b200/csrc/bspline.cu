@@ -12,7 +12,7 @@
 // (support/2).  The table itself is built on the host (bspline_functions.py).
 //
 // Forward = per (angle, block of bins) a pass over the band of pixels whose
-// taps can reach the bins, summed exactly in fixed point; adjoint = gather
+// taps can reach the bins, summed in fixed point; adjoint = gather
 // per pixel over angles and taps.  Output rows follow the angle order (no
 // reversal).
 #include <algorithm>
@@ -40,9 +40,9 @@ __device__ __forceinline__ int bs_bin(int s, float ps, double mid) {
 // Forward: a block owns kBsBins consecutive bins of one angle and slice.  Its
 // warps walk the band of pixels whose taps can reach those bins (a line per
 // warp, each pixel once) and add every tap's product lut * value, as the
-// reference rounds it, into shared-memory bins summed exactly in fixed point
-// (fixed_sum.cuh): deterministic, each bin the exact sum of the reference's
-// float products rounded once.  At most 3 pixels per line and tap reach a bin
+// reference rounds it, into shared-memory bins summed in fixed point
+// (fixed_sum.cuh): deterministic, each bin the sum of the reference's float
+// products to within the fixed-point unit, rounded once.  At most 3 pixels per line and tap reach a bin
 // (ps moves by at least 1/sqrt(2) per pixel), which bounds the sums.
 constexpr int kBsBins = 128, kBsThreads = 256;
 
@@ -83,13 +83,17 @@ __global__ void __launch_bounds__(kBsThreads) bs_forward_kernel(
     const float *__restrict__ lut, const unsigned *__restrict__ vmax, float lutmax, BsConst k, FwdEpi ep) {
   extern __shared__ float slut[];  // this angle's lut row
   __shared__ unsigned long long acc[kBsBins];
+  __shared__ unsigned flg[kBsBins];  // non-finite products per bin (fixed_sum.cuh)
   const int B0 = blockIdx.x * kBsBins, v = blockIdx.y;
   const size_t z = blockIdx.z;
   const int n = k.n;
   const float *L = lut + (size_t)v * k.lut_size;
   for (int i = threadIdx.x; i < k.lut_size; i += blockDim.x) slut[i] = __ldg(L + i);
-  for (int i = threadIdx.x; i < kBsBins; i += blockDim.x) acc[i] = 0ull;
-  // fixed-point unit: |bin| <= 3 n (2 ds + 1) max|lut| max|value|
+  for (int i = threadIdx.x; i < kBsBins; i += blockDim.x) {
+    acc[i] = 0ull;
+    flg[i] = 0u;
+  }
+  // fixed-point unit: |bin| <= 3 n (2 ds + 1) max|lut| max|finite value|
   const float vm = __uint_as_float(vmax[z]);
   const FixedScale fs = fixed_scale(3.0 * n * (2.0 * k.ds + 1.0) * (double)lutmax * (double)vm);
   __syncthreads();
@@ -131,7 +135,7 @@ __global__ void __launch_bounds__(kBsThreads) bs_forward_kernel(
         if (yi < B0 || yi >= Bend) continue;
         const int li = bs_lut_fast(yi, ps, k);
         if (li >= k.lut_max || li < 0) continue;
-        fixed_add(acc + (yi - B0), fixed_of(__fmul_rn(slut[li], val), fs));
+        fixed_add_product(acc + (yi - B0), flg + (yi - B0), __fmul_rn(slut[li], val), fs);
       }
     }
   }
@@ -139,7 +143,7 @@ __global__ void __launch_bounds__(kBsThreads) bs_forward_kernel(
   const int b = B0 + (int)threadIdx.x;
   const bool live = threadIdx.x < kBsBins && b < n;
   float out = 0.0f;
-  if (live) out = fixed_to_float(acc[threadIdx.x], fs);
+  if (live) out = flg[threadIdx.x] ? nonfinite_value(flg[threadIdx.x]) : fixed_to_float(acc[threadIdx.x], fs);
   fwd_store(ep, out, live, z * (size_t)k.na * n + (size_t)v * n + (live ? b : 0), sino);
 }
 
@@ -266,7 +270,7 @@ int bs_forward(Plan &p, const float *d_img, float *d_sino, cudaStream_t s, const
   BsState &st = *(BsState *)p.ext;
   const size_t per = (size_t)k.n * k.n;
   TOMO_CUDA(cudaMemsetAsync(st.vmax, 0, sizeof(unsigned) * p.g.nz, s));
-  fixed_absmax_kernel<<<dim3((unsigned)std::min<size_t>((per + 255) / 256, 1184), p.g.nz), 256, 0, s>>>(d_img, per,
+  fixed_finite_absmax_kernel<<<dim3((unsigned)std::min<size_t>((per + 255) / 256, 1184), p.g.nz), 256, 0, s>>>(d_img, per,
                                                                                                    st.vmax);
   dim3 fg((k.n + kBsBins - 1) / kBsBins, k.na, p.g.nz);
   bs_forward_kernel<<<fg, kBsThreads, sizeof(float) * k.lut_size, s>>>(

@@ -15,7 +15,7 @@
 // (x*s) * (1/c), and the first weight is |(t + ceil(T)) - nh|.
 //
 // Forward = per (angle, block of bins) a pass over the band of pixels whose
-// sub-samples land in the bins, summed exactly in fixed point; adjoint =
+// sub-samples land in the bins, summed in fixed point; adjoint =
 // gather per pixel over angles.  The duplicate sub-samples are evaluated once
 // with weight 2 * 1/4.
 #include <algorithm>
@@ -60,19 +60,24 @@ __device__ __forceinline__ PdEval pd_eval(float x, float y, const PdAngle &g, fl
 // warps walk the band of pixels whose sub-samples can land in (B0 - 1, Bend)
 // (a line per warp, each pixel once, along the axis on which T moves fastest)
 // and add 0.5 w value for every sub-sample and bin into shared-memory bins
-// summed exactly in fixed point (fixed_sum.cuh): deterministic, each bin the
-// exact sum of its float products rounded once.  Per line and sub-sample at
+// summed in fixed point (fixed_sum.cuh): deterministic, each bin the sum of
+// its float products to within the fixed-point unit, rounded once.  Per line and sub-sample at
 // most 3 pixels reach a bin (T moves by at least 1/sqrt(2) per pixel), so a
-// bin is bounded by 2 (sub-samples) x 3 n x 0.5 x max|image|.
+// bin is bounded by 2 (sub-samples) x 3 n x 0.5 x max|finite image value|;
+// inf and NaN products flag their bins instead (fixed_sum.cuh).
 constexpr int kPdBins = 128, kPdThreads = 256;
 
 __global__ void __launch_bounds__(kPdThreads) pd_forward_kernel(
     const float *__restrict__ img, float *__restrict__ sino, const PdAngle *__restrict__ tab,
     int n, int nh, int na, const unsigned *__restrict__ vmax, FwdEpi ep) {
   __shared__ unsigned long long acc[kPdBins];
+  __shared__ unsigned flg[kPdBins];  // non-finite products per bin (fixed_sum.cuh)
   const int B0 = blockIdx.x * kPdBins, v = blockIdx.y;
   const size_t z = blockIdx.z;
-  for (int i = threadIdx.x; i < kPdBins; i += blockDim.x) acc[i] = 0ull;
+  for (int i = threadIdx.x; i < kPdBins; i += blockDim.x) {
+    acc[i] = 0ull;
+    flg[i] = 0u;
+  }
   const FixedScale fs = fixed_scale(3.0 * n * (double)__uint_as_float(vmax[z]));
   __syncthreads();
   const PdAngle g = tab[v];
@@ -108,15 +113,16 @@ __global__ void __launch_bounds__(kPdThreads) pd_forward_kernel(
       for (int e = 0; e < 2; ++e) {
         const float d = e ? 0.25f : -0.25f;
         const PdEval q = pd_eval(__fadd_rn(x0, d), __fadd_rn(y0, d), g, fnh, n);
-        if (q.l >= B0 && q.l < Bend) fixed_add(acc + (q.l - B0), fixed_of(__fmul_rn(0.5f * q.wl, val), fs));
-        if (q.u >= B0 && q.u < Bend) fixed_add(acc + (q.u - B0), fixed_of(__fmul_rn(0.5f * q.wu, val), fs));
+        if (q.l >= B0 && q.l < Bend) fixed_add_product(acc + (q.l - B0), flg + (q.l - B0), __fmul_rn(0.5f * q.wl, val), fs);
+        if (q.u >= B0 && q.u < Bend) fixed_add_product(acc + (q.u - B0), flg + (q.u - B0), __fmul_rn(0.5f * q.wu, val), fs);
       }
     }
   }
   __syncthreads();
   const int b = B0 + (int)threadIdx.x;
   const bool live = threadIdx.x < kPdBins && b < n;
-  const float out = live ? fixed_to_float(acc[threadIdx.x], fs) : 0.0f;
+  float out = 0.0f;
+  if (live) out = flg[threadIdx.x] ? nonfinite_value(flg[threadIdx.x]) : fixed_to_float(acc[threadIdx.x], fs);
   fwd_store(ep, out, live, z * (size_t)na * n + (size_t)v * n + (live ? b : 0), sino);
 }
 
@@ -177,7 +183,7 @@ int pd_setup(Plan &p) {
   }
   TOMO_CUDA(cudaMalloc(&p.d_angles, sizeof(PdAngle) * (size_t)na));
   TOMO_CUDA(cudaMemcpy(p.d_angles, tab.data(), sizeof(PdAngle) * (size_t)na, cudaMemcpyHostToDevice));
-  // per-slice max |image| of the forward's fixed-point sums
+  // per-slice max |finite image value| of the forward's fixed-point sums
   TOMO_CUDA(cudaMalloc(&p.ext, sizeof(unsigned) * (size_t)std::max(1, p.g.nz)));
   p.ext_free = [](void *q) { cudaFree(q); };
   // residual partials of the fused solvers: one per warp of the forward launch
@@ -190,7 +196,7 @@ int pd_forward(Plan &p, const float *d_img, float *d_sino, cudaStream_t s, const
   unsigned *vmax = (unsigned *)p.ext;
   const size_t per = (size_t)n * n;
   TOMO_CUDA(cudaMemsetAsync(vmax, 0, sizeof(unsigned) * nz, s));
-  fixed_absmax_kernel<<<dim3((unsigned)std::min<size_t>((per + 255) / 256, 1184), nz), 256, 0, s>>>(d_img, per, vmax);
+  fixed_finite_absmax_kernel<<<dim3((unsigned)std::min<size_t>((per + 255) / 256, 1184), nz), 256, 0, s>>>(d_img, per, vmax);
   dim3 fg((n + kPdBins - 1) / kPdBins, na, nz);
   pd_forward_kernel<<<fg, kPdThreads, 0, s>>>(d_img, d_sino, (const PdAngle *)p.d_angles, n, p.nh, na, vmax, ep);
   TOMO_CUDA(cudaGetLastError());

@@ -16,8 +16,8 @@
 // slice) replaying its bin's five sub-rays:
 //   forward  gathers 0.2 l x[pixel] into the bin, in walk order;
 //   adjoint  scatters 0.2 l y[bin] into a 64-bit fixed-point image with
-//            integer atomics (exact, order-independent sums: deterministic),
-//            rounded to float once, through the solver epilogue, at the end.
+//            integer atomics (order-independent sums, so deterministic, of
+//            credits rounded to the fixed-point unit), rounded to float once, through the solver epilogue, at the end.
 //            Non-finite credits (inf or NaN in y, or 0 * inf) cannot be held
 //            as integers: they set per-pixel flags instead, and a flagged
 //            pixel becomes what the reference's float sum gives (+inf, -inf,
@@ -213,25 +213,10 @@ __global__ void __launch_bounds__(128) rd_forward_kernel(
   fwd_resid_commit(ep, r2, ((z * gridDim.y + v) * gridDim.x + blockIdx.x) * (blockDim.x / 32) + threadIdx.x / 32);
 }
 
-// Per slice z (blockIdx.y): out[z] = max |x| over the finite x, as float bits.
-__global__ void rd_finite_absmax_kernel(const float *__restrict__ x, size_t per_slice, unsigned *__restrict__ out) {
-  const size_t z = blockIdx.y;
-  unsigned m = 0u;
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < per_slice; i += (size_t)gridDim.x * blockDim.x) {
-    const unsigned b = __float_as_uint(fabsf(__ldg(x + z * per_slice + i)));
-    if (b < 0x7f800000u) m = max(m, b);
-  }
-  for (int off = 16; off; off >>= 1) m = max(m, __shfl_down_sync(0xffffffffu, m, off));
-  if ((threadIdx.x & 31) == 0 && m) atomicMax(out + z, m);
-}
-
-// Flags of a non-finite credit c: 1 +inf, 2 -inf, 4 NaN; set in byte p of the
-// chunk's flag array (four pixels to a 32-bit word).
-constexpr unsigned kRdPosInf = 1u, kRdNegInf = 2u, kRdNaN = 4u;
-
+// Flag bytes of non-finite credits (nonfinite_flag: 1 +inf, 2 -inf, 4 NaN),
+// byte p of the chunk's flag array for pixel p (four pixels to a 32-bit word).
 __device__ __forceinline__ void rd_flag(unsigned *flags, size_t p, float c) {
-  const unsigned f = c != c ? kRdNaN : (c > 0.0f ? kRdPosInf : kRdNegInf);
-  atomicOr(flags + (p >> 2), f << (8u * (unsigned)(p & 3)));
+  atomicOr(flags + (p >> 2), nonfinite_flag(c) << (8u * (unsigned)(p & 3)));
 }
 
 // The adjoint scatter of a bin whose value y is inf or NaN: the same walks
@@ -329,9 +314,7 @@ __global__ void rd_finalize_kernel(const unsigned long long *__restrict__ accf,
     if (live) {
       const size_t p = (size_t)R * n + C;
       const unsigned f = (flags[zl * ((per + 3) / 4) + (p >> 2)] >> (8u * (unsigned)(p & 3))) & 0xffu;
-      if (f == 0u) val = fixed_to_float(F[p] + tile[threadIdx.x][k], fs);
-      else if ((f & kRdNaN) || f == (kRdPosInf | kRdNegInf)) val = __int_as_float(0x7fffffff);
-      else val = (f & kRdPosInf) ? __int_as_float(0x7f800000) : __int_as_float(0xff800000);
+      val = f == 0u ? fixed_to_float(F[p] + tile[threadIdx.x][k], fs) : nonfinite_value(f);
     }
     adj_store(ep, val, live, ((size_t)z0 + zl) * per + (live ? (size_t)R * n + C : 0), img);
   }
@@ -413,7 +396,7 @@ int rd_adjoint(Plan &p, const float *d_sino, float *d_img, cudaStream_t s, const
   TOMO_CUDA(cudaMemsetAsync(smax, 0, sizeof(unsigned) * (size_t)nz, s));
   for (int z0 = 0; z0 < nz; z0 += chunk) {
     const int zc = std::min(chunk, nz - z0);
-    rd_finite_absmax_kernel<<<dim3(64, zc), 256, 0, s>>>(d_sino + (size_t)z0 * per_sino, per_sino, smax + z0);
+    fixed_finite_absmax_kernel<<<dim3(64, zc), 256, 0, s>>>(d_sino + (size_t)z0 * per_sino, per_sino, smax + z0);
     TOMO_CUDA(cudaMemsetAsync(accf, 0, sizeof(unsigned long long) * zc * per_img, s));
     TOMO_CUDA(cudaMemsetAsync(accT, 0, sizeof(unsigned long long) * zc * per_img, s));
     TOMO_CUDA(cudaMemsetAsync(flags, 0, sizeof(unsigned) * zc * fw, s));

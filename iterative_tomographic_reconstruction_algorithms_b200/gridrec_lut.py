@@ -15,7 +15,7 @@ Restates ``common/operators/gridrec_module/gridrec_lut.py`` of the reference:
   and outer product to a ``[nfreq, nfreq]`` matrix.
 
 The arithmetic follows the reference's numpy float32/float64 mix, so the
-arrays are the reference's to rounding (pinned in tests/test_gridrec.py).
+arrays are the reference's to rounding (pinned in tests/test_grid.py).
 """
 from __future__ import annotations
 

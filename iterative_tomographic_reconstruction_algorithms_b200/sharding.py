@@ -48,8 +48,9 @@ def slice_cost(n_op: int, na: int) -> float:
 
 def gather_to_root(results, indices, n_total: int, group=None):
     """Gathers each rank's ``results`` (one picklable object per index in
-    ``indices``) to rank 0 and returns them in slice order there (None on
-    the other ranks).  A host-side gather: the only collective of the path."""
+    ``indices``) to the group's first rank (rank 0 within ``group``) and
+    returns them in slice order there (None on the other ranks).  A host-side
+    gather: the only collective of the path."""
     import torch.distributed as dist
     if not dist.is_available() or not dist.is_initialized():
         out = [None] * n_total
@@ -60,7 +61,9 @@ def gather_to_root(results, indices, n_total: int, group=None):
     world = dist.get_world_size(group)
     payload = list(zip(indices, results))
     got = [None] * world if rank == 0 else None
-    dist.gather_object(payload, got, dst=0, group=group)
+    # gather_object takes the destination as a global rank
+    dst = 0 if group is None else dist.get_global_rank(group, 0)
+    dist.gather_object(payload, got, dst=dst, group=group)
     if rank != 0:
         return None
     out = [None] * n_total

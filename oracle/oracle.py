@@ -31,6 +31,10 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 REF_DIR = HERE / "_ref"
+# The reference source tree, read by the fixture generators, the CPU tests that
+# import the reference's own Python, and `make -C oracle ref` (its REF variable).
+# It is absent on machines that only run the GPU tests.
+REFERENCE_TREE = Path(os.environ.get("TOMO_REFERENCE_TREE", "/root/reference"))
 ORACLE_SO = HERE / "liboracle.so"
 
 _f32p = ctypes.POINTER(ctypes.c_float)
@@ -51,6 +55,24 @@ def radon_angles(angles_deg) -> np.ndarray:
     """Angle conversion of class_projectors_radon.py:49,54 (degrees -> float32 rad)."""
     a = np.asarray(angles_deg)
     return (a * np.pi / 180.0).astype(np.float32)
+
+
+def sinogram_row_of_angle(kind: str, na: int) -> np.ndarray:
+    """row[k] = the sinogram row that holds angle k (in the order passed to the
+    class) in the reference's projector output.
+
+    pd and dd shims pass ``fftshift(angles)`` to the C (radon_pixel_driven.pyx:30,
+    radon_distance_driven.pyx:27); dd and ss write angle v of their C loop to row
+    ``nang-1-v`` (radon_dd.c:181,273, radon_ss.c:111); pd and rd write row v.
+    The B-spline pair keeps the class order (gen_forwproj.c:45-75)."""
+    order = np.arange(na)
+    if kind in ("pd", "dd"):
+        order = np.fft.fftshift(order)           # C-loop index v -> class angle index
+    rows = np.empty(na, np.int64)
+    rows[order] = np.arange(na)
+    if kind in ("dd", "ss"):
+        rows = na - 1 - rows
+    return rows
 
 
 def ref_available(ref_dir: Path | None = None) -> bool:

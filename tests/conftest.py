@@ -20,7 +20,7 @@ if str(ROOT) not in sys.path:
     sys.path.insert(0, str(ROOT))
 
 GOLDEN = ROOT / "tests" / "golden"
-REFERENCE_TREE = Path("/root/reference")
+from oracle.oracle import REFERENCE_TREE  # noqa: E402,F401
 
 
 def pytest_configure(config):

@@ -24,9 +24,10 @@ import numpy as np
 
 ROOT = Path(__file__).resolve().parents[2]
 sys.path.insert(0, str(ROOT))
-REF_ALGOS = Path("/root/reference/algorithms")
 
-from oracle.oracle import Oracle, RefLib, radon_angles  # noqa: E402
+from oracle.oracle import REFERENCE_TREE, Oracle, RefLib, radon_angles  # noqa: E402
+
+REF_ALGOS = REFERENCE_TREE / "algorithms"
 from iterative_tomographic_reconstruction_algorithms_b200.phantom import random_ellipses  # noqa: E402
 
 OUT = Path(__file__).resolve().parent

@@ -23,7 +23,7 @@ import numpy as np
 ROOT = Path(__file__).resolve().parents[2]
 sys.path.insert(0, str(ROOT))
 
-from oracle.oracle import RefLib, radon_angles  # noqa: E402
+from oracle.oracle import REFERENCE_TREE, RefLib, radon_angles  # noqa: E402
 from iterative_tomographic_reconstruction_algorithms_b200.bspline_functions import init_lut_bspline  # noqa: E402
 
 OUT = Path(__file__).resolve().parent
@@ -90,7 +90,7 @@ def main() -> None:
     # errs=1e-3, 304 angles on [0, 180)), plus reference outputs on seeded inputs.
     from oracle.oracle import read_tiff_strip
     from iterative_tomographic_reconstruction_algorithms_b200 import gridrec_lut as glut
-    ref_data = Path("/root/reference/data")
+    ref_data = REFERENCE_TREE / "data"
     data = {"sl/image": read_tiff_strip(ref_data / "shepp_logan_pix0256.tif").astype(np.float32),
             "sl/sino": read_tiff_strip(ref_data / "shepp_logan_pix0256_ang0304_sino.tif")}
     for name, n, na, kernel, os_, interp, W, errs, rdeg, filt in [
@@ -133,7 +133,7 @@ def make_fbp() -> None:
     R = RefLib()
     rng = np.random.default_rng(20261203)
     spec = importlib.util.spec_from_file_location(
-        "ref_filters", "/root/reference/common/operators/filters_module/filters.py")
+        "ref_filters", REFERENCE_TREE / "common/operators/filters_module/filters.py")
     if not hasattr(np, "int"):
         np.int = int  # the reference module reads np.int at import
     ref_filters = importlib.util.module_from_spec(spec)

@@ -28,6 +28,15 @@ reconstructions are stored in ``solver_golden.npz``:
 
 ``python tests/golden/make_solver_golden.py --only em_dd`` regenerates one
 entry and keeps the others.
+
+``python tests/golden/make_solver_golden.py --c2 em`` (or ``--c2 sps``) runs the
+transmission workload at its full size instead: 512x512 phantom (seed 1) scaled
+to mu in [0, 0.02], embedded in a 768x768 operator, 720 angles on [0, 180),
+768 bins, 50 iterations of the reference ``sir.em`` (noiseless b = A mu) or
+``sir.sps`` (b from Poisson(1e4 exp(-A mu)) counts, seed 1), each in its own
+file ``solver_c2_<algo>.npz`` with the sinogram, the result and the reference's
+wall time.  One run takes about two hours on one core; the two can run at the
+same time.
 """
 from __future__ import annotations
 
@@ -40,10 +49,9 @@ from pathlib import Path
 import numpy as np
 
 ROOT = Path(__file__).resolve().parents[2]
-REF = Path("/root/reference")
 sys.path.insert(0, str(ROOT))
 
-from oracle.oracle import RefLib, radon_angles  # noqa: E402
+from oracle.oracle import REFERENCE_TREE as REF, RefLib, radon_angles  # noqa: E402
 from iterative_tomographic_reconstruction_algorithms_b200.phantom import embed, random_ellipses  # noqa: E402
 
 OUT = Path(__file__).resolve().parent / "solver_golden.npz"
@@ -113,7 +121,33 @@ def transmission_sino(tp, mu, seed, i0=1e4):
     return (-np.log(np.maximum(counts, 1) / i0)).astype(np.float32)
 
 
+def c2_transmission(algo: str) -> None:
+    """MLEM or SPS with the distance-driven pair at the full transmission size."""
+    art, sir = load_reference_solvers()
+    R = RefLib()
+    side, n_op, na = 512, 768, 720
+    deg = np.linspace(0, 180, na, endpoint=False)
+    tp = RefProjector(R, "dd", deg)
+    ph = random_ellipses(side, seed=1)
+    mu = embed(ph / max(float(ph.max()), 1e-12) * 0.02, n_op).astype(np.float32)
+    bb = (tp.A(mu) if algo == "em" else transmission_sino(tp, mu, seed=1))[None]
+    P = types.SimpleNamespace(eps=-1.0, n_iter=50, edge_padding=False, plot=False, num_cores=-1,
+                              checkit=False, projector="dist-driv", reg=None, reg_cost=0.0,
+                              huber_cost=None, index_start=0, index_end=n_op)
+    t0 = time.time()
+    x, info = getattr(sir, algo)(np.ones((1, n_op, n_op), np.float32), bb.copy(), tp, P)
+    secs = time.time() - t0
+    print(f"c2 {algo}: {secs:.1f} s")
+    out = OUT.parent / f"solver_c2_{algo}.npz"
+    np.savez_compressed(out, angles_deg=deg, b=bb[0], x50=np.asarray(x, np.float32)[0],
+                        ref_seconds=np.array([secs]))
+    print("wrote", out)
+
+
 def main() -> None:
+    if "--c2" in sys.argv:
+        c2_transmission(sys.argv[sys.argv.index("--c2") + 1])
+        return
     only = sys.argv[sys.argv.index("--only") + 1].split(",") if "--only" in sys.argv else None
     art, sir = load_reference_solvers()
     R = RefLib()

@@ -1,0 +1,97 @@
+"""Parity at the benchmarked geometry: 2048 x 2048 images, 1800 angles on
+[0, 180), 2048 bins, for every Radon kind and the B-spline pair.
+
+The GPU computes the whole 1800-angle application; the test compares the rows
+of the sampled angles (forward) and the adjoint of a sinogram that is zero
+outside those rows (at a seeded pixel sample) with the reference's outputs
+stored in tests/golden/large_golden.npz (tests/golden/make_large_golden.py),
+and with the FP64 oracle computed here on the same angles.
+
+Bars, over the sampled rows and over each row alone:
+  * against the FP64 oracle: relative L2 <= 1e-5;
+  * against the reference: relative L2 <= 1e-5 + the reference's own distance
+    from the FP64 oracle on that row.  At this size the reference's float32
+    sums of thousands of terms per bin are off the exact sums by up to 4e-5
+    (pd, phantom), 1.9e-4 (B-spline, phantom) and 3.5e-4 (dd, N(0,1) image)
+    on single rows, which no result computed in another order can reproduce;
+    on the sparse image (a few terms per bin) that floor is ~1e-7, so there
+    the bar is 1e-5 plain and pins the geometry.
+"""
+from __future__ import annotations
+
+import importlib.util
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, rel_l2
+from oracle.oracle import radon_angles, sinogram_row_of_angle
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-5
+KINDS = ("pd", "rd", "dd", "ss", "bspline")
+
+
+def load_large_fixture():
+    spec = importlib.util.spec_from_file_location("make_large_golden", GOLDEN / "make_large_golden.py")
+    mk = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mk)
+    g = np.load(GOLDEN / "large_golden.npz")
+    phantom, noise, sparse, rows, pix = mk.large_inputs()
+    sums = [x.sum(dtype=np.float64) for x in (phantom, noise, sparse, rows)]
+    assert np.array_equal(np.array(sums), g["sums"]), "seeded inputs differ from the fixture's"
+    assert np.array_equal(pix, g["pix"])
+    return mk, g, {"phantom": phantom, "noise": noise, "sparse": sparse}, rows, pix
+
+
+@pytest.fixture(scope="module")
+def large():
+    return load_large_fixture()
+
+
+def _projector(kind, n, na):
+    if kind == "bspline":
+        from iterative_tomographic_reconstruction_algorithms_b200 import class_projectors_bspline as cpb
+        return cpb.projectors(n, np.zeros(na), None), np.arange(na)
+    from iterative_tomographic_reconstruction_algorithms_b200 import class_projectors_radon as cpr
+    return cpr.projectors(n, np.linspace(0, 180, na, endpoint=False), oper=kind), sinogram_row_of_angle(kind, na)
+
+
+def _oracle(oracle, tp, kind, ang, k, x, oper):
+    if kind == "bspline":
+        return oracle.bspline(oper, x, tp.angles[k:k + 1], tp.lut[k:k + 1], tp.param_spline)
+    return oracle.radon(kind, oper, x, ang[k:k + 1])
+
+
+def _check(got, ref, orc, what):
+    floor = rel_l2(ref, orc)
+    assert rel_l2(got, orc) <= TOL, (what, "oracle", rel_l2(got, orc))
+    assert rel_l2(got, ref) <= TOL + floor, (what, "reference", rel_l2(got, ref), floor)
+
+
+@pytest.mark.parametrize("kind", KINDS)
+def test_full_geometry_sampled_angles(cuda, oracle, large, kind):
+    torch = cuda
+    mk, g, images, rows, pix = large
+    n, na = mk.N, mk.NA
+    idx = [int(k) for k in g["angle_index"]]
+    tp, rowmap = _projector(kind, n, na)
+    ang = radon_angles(np.linspace(0, 180, na, endpoint=False))
+    sel = rowmap[idx]
+
+    for name, img in images.items():
+        got = tp.A(torch.from_numpy(img).cuda()).cpu().numpy()[sel]
+        ref = g[f"{kind}/fwd_{name}"]
+        orc = np.stack([_oracle(oracle, tp, kind, ang, k, img, 0)[0] for k in idx])
+        _check(got, ref, orc, name)
+        for j, k in enumerate(idx):
+            _check(got[j], ref[j], orc[j], (name, k))
+
+    y = torch.zeros((na, n), dtype=torch.float32, device="cuda")
+    y[torch.from_numpy(sel).cuda()] = torch.from_numpy(rows).cuda()
+    adj = tp.At(y).cpu().numpy().ravel()
+    orc = np.zeros(n * n)
+    for j, k in enumerate(idx):
+        orc += _oracle(oracle, tp, kind, ang, k, rows[j:j + 1], 1).ravel()
+    assert rel_l2(adj, orc) <= TOL, ("adjoint", "oracle", rel_l2(adj, orc))
+    _check(adj[pix], g[f"{kind}/adj"], orc[pix], "adjoint")

@@ -145,3 +145,41 @@ def test_rd_adjoint_carries_non_finite_values(cuda, oracle):
     fin = np.isfinite(ref)
     assert fin.sum() > n * n // 4
     assert rel_l2(got[fin], ref[fin]) <= TOL
+
+
+def test_pd_forward_carries_non_finite_values(cuda, oracle):
+    """inf and NaN pixels reach the bins their sub-samples land in as the
+    reference's float sums carry them, and every finite bin keeps its value
+    (the fixed-point unit comes from the finite pixels only)."""
+    n, na = 64, 60
+    deg = np.linspace(0, 180, na, endpoint=False)
+    rng = np.random.default_rng(4)
+    x = rng.standard_normal((n, n)).astype(np.float32)
+    x[20, 11] = np.inf
+    x[40, 50] = -np.inf
+    x[33, 31] = np.nan
+    got = _proj("pd", n, deg).A(x)
+    ref = oracle.radon("pd", 0, x, radon_angles(deg))
+    for test in (np.isnan, np.isposinf, np.isneginf):
+        assert np.array_equal(test(got), test(ref)), test.__name__
+    fin = np.isfinite(ref)
+    assert fin.sum() > na * n // 2
+    assert rel_l2(got[fin], ref[fin]) <= TOL
+
+
+def test_bspline_forward_carries_non_finite_values(cuda, oracle):
+    from iterative_tomographic_reconstruction_algorithms_b200 import class_projectors_bspline as cpb
+    n, na = 64, 60
+    rng = np.random.default_rng(5)
+    x = rng.standard_normal((n, n)).astype(np.float32)
+    x[10, 12] = np.inf
+    x[41, 43] = -np.inf
+    x[30, 22] = np.nan
+    tp = cpb.projectors(n, np.zeros(na), None)
+    got = tp.A(x)
+    ref = oracle.bspline(0, x, tp.angles, tp.lut, tp.param_spline)
+    for test in (np.isnan, np.isposinf, np.isneginf):
+        assert np.array_equal(test(got), test(ref)), test.__name__
+    fin = np.isfinite(ref)
+    assert fin.sum() > na * n // 2
+    assert rel_l2(got[fin], ref[fin]) <= TOL

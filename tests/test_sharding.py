@@ -76,3 +76,39 @@ def test_two_rank_gloo_partition_gather_and_max():
     assert ok
     assert t == 11.0
     assert sum(sizes) == 40
+
+
+def _subgroup_worker(rank, world, port, q):
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        sub = dist.new_group([1, 2])            # a group without global rank 0
+        if rank in (1, 2):
+            costs = _costs(10, seed=3)
+            parts = lpt_partition(costs, 2)
+            mine = parts[rank - 1]
+            full = gather_to_root([i * 3 for i in mine], mine, len(costs), group=sub)
+            if rank == 1:                        # rank 0 within the group
+                q.put(full == [i * 3 for i in range(len(costs))])
+            else:
+                assert full is None
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+def test_gather_to_root_in_a_subgroup_without_global_rank_0():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_subgroup_worker, args=(r, 3, port, q)) for r in range(3)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    assert q.get(timeout=10) is True

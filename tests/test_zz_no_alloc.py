@@ -2,10 +2,11 @@
 projection for callers that cannot allocate device memory (their memory belongs
 to another allocator, or they must not allocate inside a latency-bound loop).
 
-The entry point is called through the C ABI twice in a row, on different
-inputs, and each result is compared with the plan-based forward
-(tomo_forward) within the tolerance of the other projector tests.  Also
-checked: requests beyond the static scratch are rejected with TOMO_EINVAL.
+The entry point is called through the C ABI on three inputs in a row, the
+last one filling the static scratch exactly (one 2048 x 2048 slice), and each
+result is compared with the plan-based forward (tomo_forward) and with the
+FP64 oracle within the tolerance of the other projector tests.  Also checked:
+requests beyond the static scratch are rejected with TOMO_EINVAL.
 This file sorts last so that a run stopping at the first failure has already
 run every other test; it also passes on its own in a fresh process.
 """
@@ -30,15 +31,16 @@ def _noalloc(lib, x, n, ang, nz, out, stream):
     return fn(x.data_ptr(), n, ang.ctypes.data_as(fp), len(ang), nz, out.data_ptr(), stream)
 
 
-def test_noalloc_forward_matches_plan_forward_twice(cuda):
+def test_noalloc_forward_matches_plan_forward_and_oracle(cuda, oracle):
     torch = cuda
     from iterative_tomographic_reconstruction_algorithms_b200 import _lib
     from iterative_tomographic_reconstruction_algorithms_b200.class_projectors_radon import shim_angles
     from oracle.oracle import radon_angles
     rng = np.random.default_rng(99)
     stream = torch.cuda.current_stream().cuda_stream
-    for n, na, nz in [(256, 304, 2), (193, 120, 1)]:
-        ang = shim_angles("dd", radon_angles(np.linspace(0, 180, na, endpoint=False)))
+    for n, na, nz in [(256, 304, 2), (193, 120, 1), (2048, 24, 1)]:
+        deg = np.linspace(0, 180, na, endpoint=False)
+        ang = shim_angles("dd", radon_angles(deg))
         x = torch.from_numpy(rng.standard_normal((nz, n, n)).astype(np.float32)).cuda()
         out = torch.full((nz, na, n), float("nan"), device="cuda")
         rc = _noalloc(_lib.lib, x, n, ang, nz, out, stream)
@@ -46,7 +48,11 @@ def test_noalloc_forward_matches_plan_forward_twice(cuda):
         plan = _lib.Plan(_lib.KIND_DD, n, ang, nz=nz)
         ref = plan.forward(x)
         torch.cuda.synchronize()
-        assert rel_l2(out.cpu().numpy(), ref.cpu().numpy()) <= TOL
+        got = out.cpu().numpy()
+        assert rel_l2(got, ref.cpu().numpy()) <= TOL
+        xh = x.cpu().numpy()
+        for z in range(nz):
+            assert rel_l2(got[z], oracle.radon("dd", 0, xh[z], radon_angles(deg))) <= TOL
 
 
 def test_noalloc_rejects_oversized_requests(cuda):
