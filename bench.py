@@ -52,7 +52,7 @@ def parse():
                     help="run only warm-up + steps of the device path (for ncu captures)")
     ap.add_argument("--n", type=int, default=N_SIDE, help="image side (profiling only)")
     ap.add_argument("--na", type=int, default=N_ANG, help="angle count (profiling only)")
-    ap.add_argument("--workload", default="pair", choices=["pair", "batch", "warmstart", "admm", "kinds"],
+    ap.add_argument("--workload", default="pair", choices=["pair", "batch", "warmstart", "admm", "kinds", "peaks"],
                     help="pair: the dd pair at 2048^2 x 1800 (default); batch: batched uneven SIRT; "
                          "warmstart: learned warm start, time to the plain SIRT residual")
     ap.add_argument("--train-pairs", type=int, default=256, help="warmstart: training samples")
@@ -113,6 +113,31 @@ class ClockSampler:
                     reasons.add(nm)
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx or None,
                 "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def onchip_peaks():
+    """On-chip roofline denominators measured now on the current device
+    (tomo_measure_onchip_peaks2): shared-memory 16-byte loads, L1 4-byte and
+    16-byte loads (aligned warp requests that hit L1), FP32 FMA.  ``l1_gbs`` is
+    the larger L1 rate, the one the gather kernels are measured against."""
+    import ctypes
+    from iterative_tomographic_reconstruction_algorithms_b200 import _lib
+    v = [ctypes.c_double() for _ in range(4)]
+    fn = _lib.lib.tomo_measure_onchip_peaks2
+    fn.argtypes = [ctypes.POINTER(ctypes.c_double)] * 4
+    _lib.check(fn(*[ctypes.byref(x) for x in v]), "onchip peaks")
+    smem, l1_4, l1_16, fp32 = (x.value for x in v)
+    return {"smem_gbs": smem, "l1_4_gbs": l1_4, "l1_16_gbs": l1_16, "l1_gbs": max(l1_4, l1_16),
+            "fp32_tflops": fp32}
+
+
+def run_peaks(args, rank, world, local):
+    """Only the on-chip probes (for an ncu capture of the probe kernels)."""
+    import torch
+    torch.cuda.set_device(local)
+    for _ in range(max(1, args.steps)):
+        pk = onchip_peaks()
+    print(json.dumps({"onchip_peaks": pk}), flush=True)
 
 
 def cpu_reference_gups(n: int, na_total: int, sample_angles: int, threads: int):
@@ -405,10 +430,7 @@ def run_kinds(args, rank, world, local):
     torch.cuda.set_device(dev)
     n, na = args.n, args.na
     deg = np.linspace(0, 180, na, endpoint=False)
-    s_gbs, l1_gbs, f_tf = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
-    _lib.lib.tomo_measure_onchip_peaks.argtypes = [ctypes.POINTER(ctypes.c_double)] * 3
-    _lib.check(_lib.lib.tomo_measure_onchip_peaks(ctypes.byref(s_gbs), ctypes.byref(l1_gbs), ctypes.byref(f_tf)),
-               "onchip peaks")
+    pk = onchip_peaks()
     x = torch.from_numpy(random_ellipses(n, seed=0)).to(dev)
     y = torch.from_numpy(np.random.default_rng(1).standard_normal((na, n)).astype(np.float32)).to(dev)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
@@ -443,7 +465,7 @@ def run_kinds(args, rank, world, local):
                 if kind in TAU_BYTES:
                     gbs = TAU_BYTES[kind] * n * n * na / (ms * 1e-3) / 1e9
                     r["gathered_gbs"] = gbs
-                    r["frac_of_l1"] = gbs / l1_gbs.value
+                    r["frac_of_l1"] = gbs / pk["l1_gbs"]
                 res[name] = r
             out[kind] = res
             del tp
@@ -453,7 +475,7 @@ def run_kinds(args, rank, world, local):
         "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "dtype": "f32",
         "data": "synthetic", "config": {"workload": f"each projector pair, {n}x{n} image, {na} angles [0,180), {n} bins",
                                         "l2": "flushed before every application (256 MiB write)"},
-        "kinds": out, "onchip_peaks": {"smem_gbs": s_gbs.value, "l1_gbs": l1_gbs.value, "fp32_tflops": f_tf.value},
+        "kinds": out, "onchip_peaks": pk,
         "clocks": clk.summary()}), flush=True)
 
 
@@ -497,6 +519,8 @@ def main():
         return run_admm(args, rank, world, local)
     if args.workload == "kinds":
         return run_kinds(args, rank, world, local)
+    if args.workload == "peaks":
+        return run_peaks(args, rank, world, local)
 
     import torch
     import torch.distributed as dist
@@ -525,11 +549,7 @@ def main():
         torch.cuda.synchronize()
         return
 
-    import ctypes
-    s_gbs, l1_gbs, f_tf = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
-    _lib.lib.tomo_measure_onchip_peaks.argtypes = [ctypes.POINTER(ctypes.c_double)] * 3
-    _lib.check(_lib.lib.tomo_measure_onchip_peaks(ctypes.byref(s_gbs), ctypes.byref(l1_gbs),
-                                                   ctypes.byref(f_tf)), "onchip peaks")
+    pk = onchip_peaks()
 
     def step(events=None):
         flush.fill_(1.0)
@@ -589,13 +609,14 @@ def main():
     upd_app = n * n * na
     alg_bytes = 4.0 * TAU_DD * upd_app
     achieved = alg_bytes / (dom_ms * 1e-3) / 1e9
-    peak = l1_gbs.value
+    peak = pk["l1_gbs"]
     roofline = {"bound": "l1", "kernel": f"dd_{dom}", "achieved": achieved, "peak": peak,
                 "unit": "GB/s", "frac": achieved / peak,
                 "traffic": DRAM_BYTES_PER_LAUNCH.get(dom),
                 "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one full-size launch "
                                   "(committed ncu summary of the dd pair)",
-                "peak_source": "tomo_measure_onchip_peaks (4-byte L1 loads, this run)"}
+                "peak_source": "tomo_measure_onchip_peaks2: larger of the aligned 4-byte and 16-byte L1 load "
+                               "rates, this run"}
     hbm_bytes = 4.0 * (n * n + na * n)
     peaks_file = ROOT / "MEASURED_PEAKS.json"
     hbm_peak = json.loads(peaks_file.read_text())["hbm_gbs"] if peaks_file.exists() else 6650.0
@@ -619,7 +640,7 @@ def main():
             "roofline_hbm": {"bound": "hbm", "achieved": hbm_bytes / (dom_ms * 1e-3) / 1e9,
                              "peak": hbm_peak, "unit": "GB/s",
                              "frac": hbm_bytes / (dom_ms * 1e-3) / 1e9 / hbm_peak},
-            "onchip_peaks": {"smem_gbs": s_gbs.value, "l1_gbs": l1_gbs.value, "fp32_tflops": f_tf.value},
+            "onchip_peaks": pk,
             "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},
             "clocks": clk.summary(),

@@ -81,11 +81,14 @@ int tomo_last_error(char *buf, size_t len);
 const char *tomo_version(void);
 
 /* Measures, on the current device and at its current clocks, the shared-memory
- * load bandwidth (16-byte conflict-free loads), the L1 load bandwidth (4-byte
- * loads that hit L1) and the FP32 FMA rate.  These are the roofline
- * denominators of the projector kernels (gather- and issue-bound, not HBM).
- * No reference counterpart. */
+ * load bandwidth (16-byte conflict-free loads), the L1 load bandwidth (loads
+ * that hit L1, each warp request one aligned block: 4-byte loads, one 128-byte
+ * line per request; 16-byte loads, four lines) and the FP32 FMA rate.  These
+ * are the roofline denominators of the projector kernels (gather- and
+ * issue-bound, not HBM).  tomo_measure_onchip_peaks reports the larger of the
+ * two L1 rates.  No reference counterpart. */
 int tomo_measure_onchip_peaks(double *smem_gbs, double *l1_gbs, double *fp32_tflops);
+int tomo_measure_onchip_peaks2(double *smem_gbs, double *l1_4_gbs, double *l1_16_gbs, double *fp32_tflops);
 
 /* ---- plan API ---- */
 int tomo_plan_create(const tomo_geom *geom, tomo_plan **plan);
