@@ -23,8 +23,12 @@
 //            projection: Basu & De Man, "Branchless distance driven projection
 //            and backprojection", SPIE 6065, 2006).  One table read per
 //            detector and line, however wide the detector (r = 1/|s| can be
-//            large).  Pixel widths are taken as 1; the reference's are
-//            P_j+1 - P_j in float, i.e. 1 to within an ulp of P.
+//            large).  The prefix sums take pixel widths as 1; the
+//            reference's are P_j+1 - P_j in float, which is 1 exactly except
+//            for pixels straddling a binade of P (|P| = 2^e), whose width
+//            differs by a rounding of q: those are added per line
+//            (dd_fwd_crossings).  Angles whose coordinates reach 2^22 walk
+//            the pieces instead (dd_fwd_exact).
 //   adjoint  a pixel is at most one detector wide (r >= 1), so it overlaps the
 //            detector holding its left boundary and possibly the next: two
 //            float gaps, as the reference forms them, from one 8-byte table
@@ -399,9 +403,132 @@ __device__ __forceinline__ void dd_fwd_lines(int ia, int ib, const double2 *__re
   }
 }
 
+// Boundary index of the main loop: kk = floor(D + nh + q) clamped to [-1, n],
+// computed exactly as dd_fwd_lines does (lo_nh = D + nh in float).
+__device__ __forceinline__ int dd_fwd_kk(float lo_nh, float q, float nlim) {
+  const float t = fminf(fmaxf(__fadd_rn(lo_nh, q), -0.5f), nlim);
+  return __float_as_int(__fadd_rd(t, kMagic)) - kMagicBits;
+}
+
+// Pixel widths that are not 1.  P_j = RN(x_j - q) with x_j integral: while
+// |P| < 2^23 (float spacing <= 1/2) all P_j of one binade are x_j minus the
+// same rounding of q, so P_j+1 - P_j = 1 exactly; a pixel whose boundaries
+// lie in different binades has width 1 + delta, delta the difference of two
+// roundings of q: up to 2^(e-23) at |P| ~ 2^e, i.e. 1/16 pixel at 2^19, which
+// near-axis angles reach (q = y k with |k| up to 1/|cos|).  dd_fwd_lines
+// integrates unit widths, so on each line the detector m whose boundary
+// indices bracket such a pixel j (kk_m <= j < kk_m+1, the loop's own kk) is
+// short by delta * L_j.  This adds those amounts for the item's detectors to
+// X[m - B0] (the warp's shared-memory row, zeroed by the caller).  A crossing is taken at P = +-2^e, e >= 0, each
+// pixel at the smallest one it straddles; below |P| = 1 deltas are < 2^-23.
+// Lanes take the lines of one crossing in turn; the four sums per crossing
+// (the detector holding the crossing and its neighbours) are reduced over the
+// warp in a fixed order, so the result is deterministic.
+__device__ __forceinline__ void dd_fwd_crossings(const double2 *__restrict__ SL, int ws, float k, float r, int n,
+                                                 int nh, int B0, int mEnd, int lane, double *__restrict__ X) {
+  const float DA = det_bound(B0, nh, r), DB = det_bound(mEnd, nh, r);
+  const float nlim = (float)n + 0.25f, fnh = (float)nh;
+#pragma unroll 1
+  for (int e = 0; e <= 22; ++e) {
+#pragma unroll 1
+    for (int sg = 0; sg < 2; ++sg) {
+      const float B = sg ? -ldexpf(1.0f, e) : ldexpf(1.0f, e);
+      if (!(B >= DA - 3.0f && B <= DB + 3.0f)) continue;  // warp-uniform
+      // detector holding B: D_mc <= B < D_mc+1
+      int mc = (int)floor((double)B / (double)r) + nh;
+      for (int it = 0; it < 4 && det_bound(mc, nh, r) > B; ++it) --mc;
+      for (int it = 0; it < 4 && det_bound(mc + 1, nh, r) <= B; ++it) ++mc;
+      // lines on which the crossing lies within [P_0, P_n]: q in [-nh - B - 2, n - nh - B + 2]
+      int ia, ib;
+      dd_line_range(-(double)nh - B - 2.0, (double)(n - nh) - B + 2.0, (double)k, n, nh, ia, ib);
+      double a[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll 1
+      for (int i = ia + lane; i <= ib; i += 32) {
+        const float q = __fmul_rn(__fadd_rn((float)(i - nh), 0.5f), k);
+        int j = (int)floor((double)B + (double)q) + nh - 1;
+        // j with P_j < B <= P_j+1 (B > 0) or P_j <= B < P_j+1 (B < 0)
+        if (!sg) {
+          for (int it = 0; it < 4 && pix_bound(j, nh, q) >= B; ++it) --j;
+          for (int it = 0; it < 4 && pix_bound(j + 1, nh, q) < B; ++it) ++j;
+        } else {
+          for (int it = 0; it < 4 && pix_bound(j, nh, q) > B; ++it) --j;
+          for (int it = 0; it < 4 && pix_bound(j + 1, nh, q) <= B; ++it) ++j;
+        }
+        if (j < 0 || j >= n) continue;
+        const float Pj = pix_bound(j, nh, q), Pj1 = pix_bound(j + 1, nh, q);
+        const bool at = sg ? (Pj <= B && B < Pj1 && (e == 0 || Pj1 <= 0.5f * B))
+                           : (Pj < B && B <= Pj1 && (e == 0 || Pj >= 0.5f * B));
+        if (!at) continue;
+        const float delta = __fsub_rn(__fsub_rn(Pj1, Pj), 1.0f);
+        if (delta == 0.0f) continue;
+        // the detector m with kk_m <= j < kk_m+1, among mc-1 .. mc+2
+        int m = mc;
+        for (int it = 0; it < 4; ++it) {
+          if (dd_fwd_kk(__fadd_rn(det_bound(m, nh, r), fnh), q, nlim) > j) --m;
+          else if (dd_fwd_kk(__fadd_rn(det_bound(m + 1, nh, r), fnh), q, nlim) <= j) ++m;
+          else break;
+        }
+        const double amt = (double)delta * __ldg(&SL[(size_t)i * ws + j].y);
+#pragma unroll
+        for (int t = 0; t < 4; ++t)
+          if (m == mc - 1 + t) a[t] += amt;
+      }
+#pragma unroll
+      for (int t = 0; t < 4; ++t) {
+        double v = a[t];
+        for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        const int rel = mc - 1 + t - B0;
+        if (lane == 0 && mc - 1 + t < mEnd && rel >= 0) X[rel] += v;
+      }
+      __syncwarp();
+    }
+  }
+}
+
+// An item of an angle whose pixel coordinates reach |P| >= 2^22 (|cos| or
+// |sin| ~ 1e-4, q up to nh / |cos|): there the float spacing of P is 1 or more,
+// widths are 0 or 2, and neither the unit-width integral nor its binade
+// corrections hold.  Each lane walks, for each of its detectors and each line
+// meeting it, the overlap pieces of the detector with the line's pixels, from
+// the same float boundaries as the reference, the dropped last piece skipped
+// (radon_dd.c:125-189), summed in double.
+__device__ __noinline__ void dd_fwd_exact(const double2 *__restrict__ SL, int ws, float k, float r, int n, int nh,
+                                          int B0, int mEnd, int lane, double (&T)[4]) {
+  const float Dn = det_bound(n, nh, r);
+#pragma unroll 1
+  for (int t = 0; t < 4; ++t) {
+    const int m = B0 + 32 * t + lane;
+    if (32 * t + lane >= kGrpDet || m >= mEnd) continue;
+    const float Dlo = det_bound(m, nh, r), Dhi = det_bound(m + 1, nh, r);
+    int i0, i1;
+    dd_line_range(-(double)nh - (double)Dhi, (double)(n - nh) - (double)Dlo, (double)k, n, nh, i0, i1);
+    double acc = 0.0;
+    for (int i = i0; i <= i1; ++i) {
+      const float q = __fmul_rn(__fadd_rn((float)(i - nh), 0.5f), k);
+      const float Pn = pix_bound(n, nh, q);
+      const bool lastIsPixel = Pn <= Dn;
+      const double2 *row = SL + (size_t)i * ws;
+      int kk = (int)floor((double)Dlo + (double)q + (double)nh) - 1;
+      kk = kk < 0 ? 0 : (kk > n - 1 ? n - 1 : kk);
+      float Pk = pix_bound(kk, nh, q);
+      while (kk > 0 && Pk > Dlo) Pk = pix_bound(--kk, nh, q);
+      for (; kk < n && Pk < Dhi; ++kk) {
+        const float Pk1 = pix_bound(kk + 1, nh, q);
+        const float lo = fmaxf(Pk, Dlo), hi = fminf(Pk1, Dhi);
+        if (hi > lo) {
+          const bool drop = lastIsPixel ? (kk == n - 1 && Pn <= Dhi) : (m == n - 1 && Pk1 > Dn);
+          if (!drop) acc += (double)__fsub_rn(hi, lo) * __ldg(&row[kk].y);
+        }
+        Pk = Pk1;
+      }
+    }
+    T[t] = acc;
+  }
+}
+
 __device__ __forceinline__ void dd_fwd_item(const DdInst &I, int v, int grp, int lane,
                                             const double2 *__restrict__ work, float *__restrict__ sino,
-                                            const FwdEpi &ep, long long slot) {
+                                            const FwdEpi &ep, long long slot, double *__restrict__ xs) {
   const DdAngle g = I.ang[v];
   const int n = I.n, nh = I.nh, ws = n + 2;
   const int B0 = grp * kGrpDet;
@@ -437,17 +564,29 @@ __device__ __forceinline__ void dd_fwd_item(const DdInst &I, int v, int grp, int
       j0 = i1 + 1;
       j1 = i1;
     }
-    double T[4] = {0.0, 0.0, 0.0, 0.0}, C[4] = {0.0, 0.0, 0.0, 0.0};
-    dd_fwd_lines<false>(i0, j0, SL, ws, k, r, n, nh, B0, lane, Dlo, lo_nh, T, C);
-    dd_fwd_lines<true>(j0, j1 + 1, SL, ws, k, r, n, nh, B0, lane, Dlo, lo_nh, T, C);
-    dd_fwd_lines<false>(j1 + 1, i1 + 1, SL, ws, k, r, n, nh, B0, lane, Dlo, lo_nh, T, C);
-    // the upper boundary of detector B0 + 32 j + l is lane l+1's j-th, or lane 0's (j+1)-th
+    if (fabsf(k) * (float)(nh + 1) + (float)(nh + 2) >= 4194304.0f) {
+      // |P| reaches 2^22: pieces walked exactly (rare near-axis angles)
+      double T[4] = {0.0, 0.0, 0.0, 0.0};
+      dd_fwd_exact(SL, ws, k, r, n, nh, B0, mEnd, lane, T);
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const double a = __shfl_down_sync(0xffffffffu, T[j], 1);
-      const double b = __shfl_sync(0xffffffffu, j < 3 ? T[j < 3 ? j + 1 : 3] : 0.0, 0);
-      const double up = lane < 31 ? a : b;
-      acc[j] = (float)((up - T[j]) - C[j]);
+      for (int j = 0; j < 4; ++j) acc[j] = (float)T[j];
+    } else {
+#pragma unroll
+      for (int j = 0; j < 4; ++j) xs[32 * j + lane] = 0.0;
+      __syncwarp();
+      dd_fwd_crossings(SL, ws, k, r, n, nh, B0, mEnd, lane, xs);
+      double T[4] = {0.0, 0.0, 0.0, 0.0}, C[4] = {0.0, 0.0, 0.0, 0.0};
+      dd_fwd_lines<false>(i0, j0, SL, ws, k, r, n, nh, B0, lane, Dlo, lo_nh, T, C);
+      dd_fwd_lines<true>(j0, j1 + 1, SL, ws, k, r, n, nh, B0, lane, Dlo, lo_nh, T, C);
+      dd_fwd_lines<false>(j1 + 1, i1 + 1, SL, ws, k, r, n, nh, B0, lane, Dlo, lo_nh, T, C);
+      // the upper boundary of detector B0 + 32 j + l is lane l+1's j-th, or lane 0's (j+1)-th
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const double a = __shfl_down_sync(0xffffffffu, T[j], 1);
+        const double b = __shfl_sync(0xffffffffu, j < 3 ? T[j < 3 ? j + 1 : 3] : 0.0, 0);
+        const double up = lane < 31 ? a : b;
+        acc[j] = (float)(((up - T[j]) - C[j]) + xs[32 * j + lane]);
+      }
     }
   }
   double r2 = 0.0;
@@ -486,11 +625,12 @@ __device__ __forceinline__ int centre_out(int gi, int ngrp) {
 }
 
 template <int W, bool BLOCK>
-__global__ void __launch_bounds__(32 * W) dd_fwd_kernel(const DdInst *__restrict__ inst, int ninst,
+__global__ void __launch_bounds__(32 * W, 28 / W) dd_fwd_kernel(const DdInst *__restrict__ inst, int ninst,
                                                          long long nitems, unsigned long long *__restrict__ ctr,
                                                          const double2 *__restrict__ work,
                                                          float *__restrict__ sino, FwdEpi ep) {
   __shared__ long long base_s;
+  __shared__ double xs[W][128];  // per warp: binade corrections of its item's detectors
   const int lane = threadIdx.x & 31;
   for (;;) {
     const long long item = fetch_item<BLOCK>(ctr, W, &base_s);
@@ -498,7 +638,8 @@ __global__ void __launch_bounds__(32 * W) dd_fwd_kernel(const DdInst *__restrict
     if (item < nitems) {
       const DdInst &I = inst[find_inst(inst, ninst, item, &DdInst::f0)];
       const int local = (int)(item - I.f0);
-      dd_fwd_item(I, local % I.na, centre_out(local / I.na, I.ngrp), lane, work, sino, ep, item);
+      dd_fwd_item(I, local % I.na, centre_out(local / I.na, I.ngrp), lane, work, sino, ep, item,
+                  xs[threadIdx.x >> 5]);
     }
   }
 }

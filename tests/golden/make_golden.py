@@ -28,13 +28,19 @@ from iterative_tomographic_reconstruction_algorithms_b200.bspline_functions impo
 
 OUT = Path(__file__).resolve().parent
 
-# (name, n, angle set in degrees)
+# (name, n, angle set in degrees[, own seed]); cases with their own seed draw
+# their inputs from a separate generator, so adding one leaves the others as
+# they were
 RADON_CASES = [
     ("n64_a90", 64, np.linspace(0, 180, 90, endpoint=False)),
     ("n65_a37", 65, np.linspace(0, 180, 37, endpoint=False)),
     ("n48_special", 48, np.array([0.0, 30.0, 45.0, 60.0, 90.0, 120.0, 135.0, 150.0, 179.5])),
     ("n33_a16", 33, np.linspace(0, 180, 16, endpoint=False)),
     ("n128_a45", 128, np.linspace(0, 180, 45, endpoint=False)),
+    # near-axis angles: pixel coordinates up to nh / |cos| (binade crossings of
+    # P with large width errors; beyond 2^22 the widths are 0 or 2)
+    ("n256_nearaxis", 256, np.array([0.1, 0.5, 44.9, 89.5, 89.9, 89.99, 89.999, 90.001, 90.1, 134.9,
+                                     179.5, 179.9, 179.99, 179.999]), 256),
 ]
 
 
@@ -42,11 +48,12 @@ def main() -> None:
     R = RefLib()
     rng = np.random.default_rng(20240611)
     data = {}
-    for name, n, deg in RADON_CASES:
+    for name, n, deg, *own in RADON_CASES:
         ang = radon_angles(deg)
         na = len(ang)
-        img = rng.standard_normal((n, n)).astype(np.float32)
-        sino = rng.standard_normal((na, n)).astype(np.float32)
+        g = np.random.default_rng(own[0]) if own else rng
+        img = g.standard_normal((n, n)).astype(np.float32)
+        sino = g.standard_normal((na, n)).astype(np.float32)
         data[f"{name}/angles_deg"] = deg.astype(np.float64)
         data[f"{name}/image"] = img
         data[f"{name}/sino"] = sino
@@ -64,6 +71,8 @@ def main() -> None:
             data[f"{name}/{kind}/fwd"] = R.radon(kind, 0, img, ang)
             data[f"{name}/{kind}/adj"] = R.radon(kind, 1, sino, ang)
     np.savez_compressed(OUT / "radon_golden.npz", **data)
+    if "--radon-only" in sys.argv:
+        return
 
     data = {}
     for name, n, na, deg, sup in [("n64_a90_cubic", 64, 90, 3, 4.0), ("n65_a37_cubic", 65, 37, 3, 4.0),
@@ -186,4 +195,5 @@ if __name__ == "__main__":
         make_fbp()
     else:
         main()
-        make_fbp()
+        if "--radon-only" not in sys.argv:
+            make_fbp()
