@@ -13,11 +13,19 @@ slices (independent slices: weak scaling, no collective on the data path);
 the step time is the max over ranks.  ``--impl reference`` times the
 reference's own C kernel (compiled into oracle/_ref) on the host cores, on a
 bounded sample of angles of the same workload.
+
+At N = 1 the line also carries ``blocks``: the other configurations, each
+measured after the headline in the same process (C1 SIRT + ray-driven pair,
+C2 MLEM / SPS + distance-driven pair against the reference's own results,
+C3 ADMM-TV + gridding with the gridding roofline, C4 batched uneven SIRT over
+512 slices, C5 learned warm start trained and evaluated here).  They take a
+few minutes; ``--no-blocks`` skips them.
 """
 from __future__ import annotations
 
 import argparse
 import json
+import math
 import os
 import subprocess
 import sys
@@ -55,9 +63,13 @@ def parse():
     ap.add_argument("--workload", default="pair", choices=["pair", "batch", "warmstart", "admm", "kinds", "peaks"],
                     help="pair: the dd pair at 2048^2 x 1800 (default); batch: batched uneven SIRT; "
                          "warmstart: learned warm start, time to the plain SIRT residual")
-    ap.add_argument("--train-pairs", type=int, default=256, help="warmstart: training samples")
-    ap.add_argument("--train-steps", type=int, default=2000, help="warmstart: training steps")
-    ap.add_argument("--eval-slices", type=int, default=16, help="warmstart: held-out slices")
+    ap.add_argument("--train-pairs", type=int, default=1024, help="warmstart: training samples")
+    ap.add_argument("--train-steps", type=int, default=1500, help="warmstart: training steps")
+    ap.add_argument("--eval-slices", type=int, default=128, help="warmstart: held-out slices")
+    ap.add_argument("--no-blocks", action="store_true",
+                    help="pair workload: skip the C1-C5 blocks measured after the headline")
+    ap.add_argument("--block-slices", type=int, default=512, help="C4 block: slices")
+    ap.add_argument("--block-iters", type=int, default=5, help="C4 block: SIRT iterations timed")
     ap.add_argument("--lam", type=float, default=0.03, help="warmstart: weight of the data-consistency loss")
     ap.add_argument("--slices", type=int, default=64, help="batch workload: number of slices")
     ap.add_argument("--no-cpu-baseline", action="store_true", help="admm workload: skip the host reference sample")
@@ -140,11 +152,26 @@ def run_peaks(args, rank, world, local):
     print(json.dumps({"onchip_peaks": pk}), flush=True)
 
 
+def sample_angle_index(na_total: int, sample_angles: int) -> np.ndarray:
+    """``sample_angles`` indices into the reference's (fftshifted) angle order,
+    evenly spread over the angles that take the general path: the axis angles
+    (|sin| or |cos| < 1e-7, plain row / column sums, radon_dd.c:75-96) are left
+    out, so each sampled angle costs what a general angle costs."""
+    from oracle.oracle import radon_angles
+    from iterative_tomographic_reconstruction_algorithms_b200.phantom import angles_deg
+    a = np.fft.fftshift(radon_angles(angles_deg(na_total))).astype(np.float64)
+    general = np.nonzero((np.abs(np.sin(a)) >= 1e-7) & (np.abs(np.cos(a)) >= 1e-7))[0]
+    return general[np.linspace(0, len(general) - 1, sample_angles).astype(int)]
+
+
 def cpu_reference_gups(n: int, na_total: int, sample_angles: int, threads: int):
     """Reference dd kernel (oracle/_ref/ref_dd.so) on a sample of the angles.
 
     Returns (GUPS, seconds, description).  ``threads`` > 1 runs that many
     angle chunks concurrently (ctypes releases the GIL during the C call).
+    The rate is that of the general angles; the two axis angles of 1800 (row
+    and column sums) are cheaper, so the whole application's rate is higher by
+    about 0.1 %.
     """
     from concurrent.futures import ThreadPoolExecutor
 
@@ -152,7 +179,7 @@ def cpu_reference_gups(n: int, na_total: int, sample_angles: int, threads: int):
     from iterative_tomographic_reconstruction_algorithms_b200.phantom import angles_deg, random_ellipses
     R = RefLib()
     ang_all = radon_angles(angles_deg(na_total))
-    idx = np.linspace(0, na_total - 1, sample_angles).astype(int)
+    idx = sample_angle_index(na_total, sample_angles)
     ang = np.ascontiguousarray(np.fft.fftshift(ang_all)[idx])
     img = random_ellipses(n, seed=0)
     chunks = np.array_split(np.arange(len(ang)), threads)
@@ -179,7 +206,8 @@ def cpu_reference_gups(n: int, na_total: int, sample_angles: int, threads: int):
     dt = time.perf_counter() - t0
     updates = 2.0 * n * n * len(ang)
     desc = (f"reference radon_dd (oracle/_ref, -O3 -ffast-math) forward+adjoint on {len(ang)} of "
-            f"{na_total} angles at {n}x{n}, {threads} thread(s)")
+            f"{na_total} angles at {n}x{n} (evenly spread over the non-axis angles), {threads} thread(s); "
+            f"rate extrapolated to the whole application")
     return updates / dt / 1e9, dt, desc
 
 
@@ -187,7 +215,7 @@ def run_reference(args, rank, world):
     if rank != 0:
         return
     threads = os.cpu_count() or 1
-    sample = args.cpu_sample_angles or max(threads, 8)
+    sample = args.cpu_sample_angles or max(4 * threads, 64)
     vals = []
     for i in range(args.warmup + args.steps):
         g, dt, desc = cpu_reference_gups(N_SIDE, N_ANG, sample, threads)
@@ -205,32 +233,27 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
-def run_batch(args, rank, world, local):
+def batch_core(n_slices, iters, steps, warmup, rank, world, dev):
     """Batched uneven SIRT: slices of side 256/512/1024/2048 (weights 4:3:2:1, seeded
     draw), round(1.5 side) angles on [0, 180), ceil(1.5 side) bins (the operator side;
     the phantom is centred in it), noiseless data from the same projector.  All
     slices form one batched plan: every projector application is one persistent
-    launch, every iteration one CUDA-graph replay.  A step is ``--iters`` SIRT
+    launch, every iteration one CUDA-graph replay.  A step is ``iters`` SIRT
     iterations of every slice; the metric counts 2 n_op^2 na updates per slice and
-    iteration."""
+    iteration.  With world > 1 the slice list (n_slices per rank) is split across
+    ranks by LPT on cost.  Returns the result fields (rank 0) and the step time."""
     import math
 
     import torch
     from iterative_tomographic_reconstruction_algorithms_b200 import _lib
     from iterative_tomographic_reconstruction_algorithms_b200.class_projectors_radon import shim_angles
     from iterative_tomographic_reconstruction_algorithms_b200.phantom import embed, random_ellipses
-    from iterative_tomographic_reconstruction_algorithms_b200.solvers import Solver
-    import torch.distributed as dist
-    dev = torch.device("cuda", local)
-    torch.cuda.set_device(dev)
-    if world > 1:
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
     from iterative_tomographic_reconstruction_algorithms_b200.sharding import (lpt_partition, max_over_ranks,
                                                                                slice_cost)
-    # one slice list for the whole job (--slices per rank), split across ranks by LPT on cost
+    from iterative_tomographic_reconstruction_algorithms_b200.solvers import Solver
+    import torch.distributed as dist
     rng = np.random.default_rng(4)
-    all_sides = rng.choice([256, 512, 1024, 2048], size=args.slices * world, p=[0.4, 0.3, 0.2, 0.1])
+    all_sides = rng.choice([256, 512, 1024, 2048], size=n_slices * world, p=[0.4, 0.3, 0.2, 0.1])
     costs = [slice_cost(int(math.ceil(1.5 * s)), int(round(1.5 * s))) for s in all_sides]
     mine = lpt_partition(costs, world)[rank]
     sides = all_sides[mine]
@@ -245,82 +268,138 @@ def run_batch(args, rank, world, local):
     b = bp.forward(x_true)
     solver = Solver(bp, "sirt", b)
     x0 = torch.ones(bp.img_total, device=dev)
-    for _ in range(max(1, args.warmup)):
+    for _ in range(max(1, warmup)):
         solver.run(x0, 1)
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local) as clk:
+    with ClockSampler(dev.index) as clk:
         ev0.record()
-        for _ in range(args.steps):
-            x, res = solver.run(x0, args.iters)
+        for _ in range(steps):
+            x, res = solver.run(x0, iters)
         ev1.record()
         torch.cuda.synchronize()
-    ms = max_over_ranks(ev0.elapsed_time(ev1) / args.steps)
-    upd = float(sum(2.0 * c for c in costs)) * args.iters
+    ms = max_over_ranks(ev0.elapsed_time(ev1) / steps)
+    upd = float(sum(2.0 * c for c in costs)) * iters
+    out = {"value": upd / (ms * 1e-3) / 1e9, "unit": "GUPS", "ms_per_step": ms,
+           "config": {"workload": f"{n_slices * world} slices, sides {{256,512,1024,2048}} weights 4:3:2:1, "
+                                  f"na=round(1.5 side), nb=ceil(1.5 side), {iters} SIRT iterations per step",
+                      "sides": {int(s): int((all_sides == s).sum()) for s in (256, 512, 1024, 2048)},
+                      "slices_total": int(len(all_sides)), "sharding": "LPT on n_op^2 na, no data-path collective",
+                      "updates_per_step": upd, "instances": bp.instances},
+           "residual_first_last": [float(res[0]), float(res[-1])],
+           "tuning": bp.tuning(), "clocks": clk.summary()}
+    del solver, bp, x_true, b
+    torch.cuda.empty_cache()
+    return out
+
+
+def run_batch(args, rank, world, local):
+    """The batched uneven SIRT workload (batch_core) as its own bench line."""
+    import torch
+    import torch.distributed as dist
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
+    r = batch_core(args.slices, args.iters, args.steps, args.warmup, rank, world, dev)
     if rank == 0:
-        print(json.dumps({
-            "metric": "batched SIRT GUPS (pixel x angle updates per second, uneven slices, one launch per application)",
-            "value": upd / (ms * 1e-3) / 1e9, "unit": "GUPS", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"{args.slices} slices, sides {{256,512,1024,2048}} weights 4:3:2:1, "
-                                   f"na=round(1.5 side), nb=ceil(1.5 side), {args.iters} SIRT iterations per step",
-                       "sides": {int(s): int((all_sides == s).sum()) for s in (256, 512, 1024, 2048)},
-                       "slices_total": int(len(all_sides)), "sharding": "LPT on n_op^2 na, no data-path collective",
-                       "updates_per_step": upd, "instances": bp.instances},
-            "residual_first_last": [float(res[0]), float(res[-1])],
-            "tuning": bp.tuning(), "clocks": clk.summary()}), flush=True)
+        line = {"metric": "batched SIRT GUPS (pixel x angle updates per second, uneven slices, one launch per application)",
+                "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic"}
+        line.update(r)
+        print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
 
 
-def run_warmstart(args, rank, world, local):
+def oracle_residuals(xs, b, na, threads=None):
+    """||A x - b||^2 per slice with the FP64 oracle's distance-driven forward
+    (float32 geometry, float64 sums), one angle per call in a thread pool;
+    b in the class's row order (sinogram_row_of_angle)."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    from oracle.oracle import Oracle, radon_angles, sinogram_row_of_angle
+    orc = Oracle()
+    ang = radon_angles(np.linspace(0, 180, na, endpoint=False))
+    rows = sinogram_row_of_angle("dd", na)
+    out = []
+    for x, bb in zip(xs, b):
+        x = np.ascontiguousarray(x, np.float32)
+        bb = np.asarray(bb, np.float64)
+
+        def one(k):
+            r = orc.radon("dd", 0, x, ang[k:k + 1])[0]
+            return float(((r - bb[rows[k]]) ** 2).sum())
+
+        with ThreadPoolExecutor(max_workers=threads or os.cpu_count() or 1) as ex:
+            out.append(float(sum(ex.map(one, range(na)))))
+    return out
+
+
+def warmstart_core(train_pairs, train_steps, eval_slices, lam, dev, oracle_slices=2):
     """Learned warm start at 512^2 (768 bins), 180 angles on [0, 180), Poisson I0 = 5e3:
     samples (2-iteration SIRT, filtered backprojection, 300-iteration SIRT, phantom)
     generated by the batched solver on seeds 10000 + i, a 4-level, 32-channel U-Net
     trained on them with the tensor-core kernels, then on held-out seeds 100000 + i the
     GPU time plain SIRT needs for its 300 iterations against the time the warm start
     (2 iterations + network + fallback check + SIRT) needs to reach the same data
-    residual.  Metric: warm / plain time (lower is better)."""
+    residual.  The final data residuals of ``oracle_slices`` held-out slices are also
+    computed with the FP64 oracle.  Metric: warm / plain time (lower is better)."""
     import torch
     from iterative_tomographic_reconstruction_algorithms_b200 import nn, warmstart as ws
-    dev = torch.device("cuda", local)
-    torch.cuda.set_device(dev)
     pb = ws.Problem()
     t0 = time.perf_counter()
-    data = ws.make_pairs(pb, [10000 + i for i in range(args.train_pairs)])
+    data = ws.make_pairs(pb, [10000 + i for i in range(train_pairs)])
     torch.cuda.synchronize()
     t_pairs = time.perf_counter() - t0
     net = nn.UNet(levels=4, base=32, seed=0).to(dev)
     t0 = time.perf_counter()
-    hist = ws.train(net, pb, data, steps=args.train_steps, batch=4, lam=args.lam)
+    hist = ws.train(net, pb, data, steps=train_steps, batch=4, lam=lam)
     torch.cuda.synchronize()
     t_train = time.perf_counter() - t0
     del data
-    r = ws.time_to_residual(net, pb, [100000 + i for i in range(args.eval_slices)])
+    torch.cuda.empty_cache()
+    r = ws.time_to_residual(net, pb, [100000 + i for i in range(eval_slices)])
+    k = min(oracle_slices, eval_slices)
+    bh = r["b"][:k].cpu().numpy()
+    res_p = oracle_residuals(r["x_plain"][:k].cpu().numpy(), bh, pb.na)
+    res_w = oracle_residuals(r["x_warm"][:k].cpu().numpy(), bh, pb.na)
+    out = {"value": r["ratio"], "unit": "ratio (warm / plain GPU time)", "higher_is_better": False,
+           "config": {"workload": "512^2 phantom in 768 bins, 180 angles, Poisson I0=5e3, dd pair, SIRT from 0; "
+                                  "U-Net 4 levels x 32 channels, BF16 weights/activations, FP32 accumulation",
+                      "train_pairs": train_pairs, "train_steps": train_steps, "lam": lam,
+                      "eval_slices": eval_slices},
+           "plain_ms": r["plain_ms"], "warm_ms": r["warm_ms"], "warm_iters": r["warm_iters"],
+           "plain_iters": r["plain_iters"], "residual_plain": r["residual_plain"],
+           "residual_warm": r["residual_warm"], "image_rel_err_plain": r["err_plain"],
+           "image_rel_err_warm": r["err_warm"], "image_rel_err_start": r["err_start"],
+           "fallback_slices": r["fallback_slices"],
+           "fp64_oracle_residual": {"slices": k, "plain": res_p, "warm": res_w},
+           "pairs_s": t_pairs, "train_s": t_train, "loss_first_last": [hist[0], hist[-1]] if hist else None}
+    del r, net
+    torch.cuda.empty_cache()
+    return out
+
+
+def run_warmstart(args, rank, world, local):
+    """The learned warm start (warmstart_core) as its own bench line."""
+    import torch
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    r = warmstart_core(args.train_pairs, args.train_steps, args.eval_slices, args.lam, dev)
     if rank == 0:
-        print(json.dumps({
-            "metric": "learned warm start: GPU time to reach plain SIRT's 300-iteration data residual, warm / plain",
-            "value": r["ratio"], "unit": "ratio", "n_gpus": 1, "steps": 1, "warmup": 1,
-            "ms_per_step": r["warm_ms"], "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
-            "dtype": "bf16 network (fp32 accumulation), f32 projector", "data": "synthetic",
-            "config": {"workload": "512^2 phantom in 768 bins, 180 angles, Poisson I0=5e3, dd pair, SIRT from 0; "
-                                   "U-Net 4 levels x 32 channels",
-                       "train_pairs": args.train_pairs, "train_steps": args.train_steps, "lam": args.lam,
-                       "eval_slices": args.eval_slices},
-            "plain_ms": r["plain_ms"], "warm_ms": r["warm_ms"], "warm_iters": r["warm_iters"],
-            "plain_iters": r["plain_iters"], "residual_plain": r["residual_plain"],
-            "residual_warm": r["residual_warm"], "image_rel_err_plain": r["err_plain"],
-            "image_rel_err_warm": r["err_warm"], "image_rel_err_start": r["err_start"],
-            "fallback_slices": r["fallback_slices"], "residual_start": r["residual_start"],
-            "residual_curve_plain": r["residual_curve_plain"], "warm_curve": r["warm_curve"],
-            "pairs_s": t_pairs, "train_s": t_train, "loss_history": hist}), flush=True)
+        line = {"metric": "learned warm start: GPU time to reach plain SIRT's 300-iteration data residual, warm / plain",
+                "n_gpus": 1, "steps": 1, "warmup": 1, "ms_per_step": r["warm_ms"], "scaling": "weak",
+                "vs_baseline": None, "dtype": "bf16 network (fp32 accumulation), f32 projector", "data": "synthetic"}
+        line.update(r)
+        print(json.dumps(line), flush=True)
 
 
-def run_admm(args, rank, world, local):
+def admm_core(steps, warmup, dev, cpu_baseline=True):
     """ADMM-TV (admm.lasso_tv) with the gridding pair: 1024^2 phantom centred in
     1536 bins, 1500 angles on [0, 180), Kaiser-Bessel W = 6, oversampling 2
     (4096^2 Fourier grid), linear interpolation, b = A x + Gaussian noise of
@@ -333,8 +412,6 @@ def run_admm(args, rank, world, local):
     from iterative_tomographic_reconstruction_algorithms_b200 import admm as ad
     from iterative_tomographic_reconstruction_algorithms_b200 import class_projectors_grid as cpg
     from iterative_tomographic_reconstruction_algorithms_b200.phantom import embed, random_ellipses
-    dev = torch.device("cuda", local)
-    torch.cuda.set_device(dev)
     n, na, side = 1536, 1500, 1024
     deg = np.linspace(0, 180, na, endpoint=False)
     tp = cpg.projectors(n, deg, kernel="kb", oversampl=2.0, W=6.0, errs=1e-3, interp="lin", verbose=False)
@@ -345,16 +422,16 @@ def run_admm(args, rank, world, local):
     l1, l2, mu, n2 = 0.1, 1.0, 20.0, 5
     solver = ad.AdmmSolver(tp, "lasso-tv", b, l1, l2, mu, n2)
     x = torch.ones((1, n, n), device=dev)
-    solver.run(x, max(1, args.warmup), reset=True)
+    solver.run(x, max(1, warmup), reset=True)
     torch.cuda.synchronize()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     stream = torch.cuda.current_stream(dev)
-    with ClockSampler(local) as clk:
+    with ClockSampler(dev.index) as clk:
         ev0.record(stream)
-        st = solver.run(x, args.steps, reset=False)
+        st = solver.run(x, steps, reset=False)
         ev1.record(stream)
         torch.cuda.synchronize()
-    ms = ev0.elapsed_time(ev1) / args.steps
+    ms = ev0.elapsed_time(ev1) / steps
     # the projector pairs alone (6 per outer iteration), same stream
     plan = tp.plan(1, dev.index)
     sino = plan.forward(x)
@@ -376,17 +453,31 @@ def run_admm(args, rank, world, local):
     bh = b.cpu().numpy()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    ad.lasso_tv(xh, bh, tp, ad.Param(lambd1=l1, lambd2=l2, mu=mu, n_iter=args.steps, n_iter_pcg=n2), track=False)
+    ad.lasso_tv(xh, bh, tp, ad.Param(lambd1=l1, lambd2=l2, mu=mu, n_iter=steps, n_iter_pcg=n2), track=False)
     torch.cuda.synchronize()
-    e2e_ms = (time.perf_counter() - t0) * 1e3 / args.steps
+    e2e_ms = (time.perf_counter() - t0) * 1e3 / steps
     rel = float((x[0].double() - x_true.double()).norm() / x_true.double().norm())
     cpu = None
-    if not args.no_cpu_baseline:
+    if cpu_baseline:
         cpu = admm_cpu_baseline(tp, b[0].cpu().numpy(), n, n2)
     upd = 12.0 * n * n * na  # 6 pairs of n^2 na updates per outer iteration
+    # gridding roofline: per application na * pdim polar samples (both half-planes), each a
+    # ceil(lconv)^2 window of complex64 taps (8 B and 8 flops a tap), plus the 2-D FFT
+    # (5 pdim^2 log2(pdim^2) flops); peaks: L1 16-byte loads and FP32 FMA, measured now
+    pk = onchip_peaks()
+    from iterative_tomographic_reconstruction_algorithms_b200.gridrec_lut import grid_size
+    pdim = grid_size(n, 2.0)
+    roof = {}
+    for name, lconv, t_ms in (("forward", 2 * 7.0 / np.pi, fwd_ms), ("adjoint", float(tp.param_nofilt[6]), adj_ms)):
+        taps = float(na) * pdim * math.ceil(lconv) ** 2
+        flops = 8.0 * taps + 5.0 * pdim * pdim * math.log2(pdim * pdim)
+        gb = 8.0 * taps / (t_ms * 1e-3) / 1e9
+        tf = flops / (t_ms * 1e-3) / 1e12
+        roof[name] = {"ms": t_ms, "window": math.ceil(lconv), "gathered_gbs": gb, "frac_of_l1": gb / pk["l1_gbs"],
+                      "tflops": tf, "frac_of_fp32": tf / pk["fp32_tflops"]}
     out = {
         "metric": "ADMM-TV outer iterations per second (gridding pair, 5 inner CG iterations)",
-        "value": 1e3 / ms, "unit": "iterations/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "value": 1e3 / ms, "unit": "iterations/s", "n_gpus": 1, "steps": steps, "warmup": warmup,
         "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f64 CG r, p)",
         "data": "synthetic",
         "config": {"workload": "ADMM-TV, 1024^2 phantom in 1536 bins, 1500 angles, gridding KB W=6 os=2 lin, "
@@ -396,12 +487,135 @@ def run_admm(args, rank, world, local):
         "forward_ms": fwd_ms, "adjoint_ms": adj_ms,
         "pair_gups": upd / (pairs_ms * 1e-3) / 1e9,
         "err_last": float(np.sqrt(st[-1, :, 0].sum())), "image_rel_err_after_all_steps": rel,
-        "e2e": {"value": 1e3 / e2e_ms, "unit": "iterations/s", "h2d_bytes_per_step": 4 * (n * n + na * n) / args.steps,
-                "d2h_bytes_per_step": 4 * n * n / args.steps},
-        "gpu_launches": None, "clocks": clk.summary()}
+        "e2e": {"value": 1e3 / e2e_ms, "unit": "iterations/s", "h2d_bytes_per_step": 4 * (n * n + na * n) / steps,
+                "d2h_bytes_per_step": 4 * n * n / steps},
+        "gridding_roofline": roof, "clocks": clk.summary()}
     if cpu is not None:
         out["cpu_baseline"] = cpu
-    print(json.dumps(out), flush=True)
+    del solver
+    torch.cuda.empty_cache()
+    return out
+
+
+def run_admm(args, rank, world, local):
+    """The ADMM-TV workload (admm_core) as its own bench line."""
+    import torch
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    print(json.dumps(admm_core(args.steps, args.warmup, dev, not args.no_cpu_baseline)), flush=True)
+
+
+def c1_core(dev, cpu=True):
+    """C1: SIRT with the ray-driven pair, 256 x 256, 304 angles on [0, 180), 100
+    iterations from x0 = 1, on the noiseless sinogram of a random-ellipse phantom
+    (seed 0) that the reference projector made (tests/golden/solver_golden.npz).
+    GPU: the fused solver's 100 iterations under CUDA events; parity: relative L2
+    of x_100 to the reference's own art.sirt result in that fixture.  CPU: the
+    reference rd kernel timed once forward and once adjoint at this size, scaled
+    to 100 iterations of two forward and one adjoint application each
+    (art.py:226-236 and the objective's forward, :326)."""
+    import torch
+    from iterative_tomographic_reconstruction_algorithms_b200 import class_projectors_radon as cpr
+    from iterative_tomographic_reconstruction_algorithms_b200.solvers import Solver
+    g = np.load(ROOT / "tests" / "golden" / "solver_golden.npz")
+    deg, b, xref = g["sirt_rd/angles_deg"], g["sirt_rd/b"], g["sirt_rd/x100"]
+    n = b.shape[1]
+    tp = cpr.projectors(n, deg, oper="rd")
+    solver = Solver(tp, "sirt", b)
+    x0 = torch.ones((1, n, n), device=dev)
+    solver.run(x0, 1)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    x, _ = solver.run(x0, 100)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    xh = x[0].cpu().numpy().astype(np.float64)
+    rel = float(np.linalg.norm(xh - xref) / np.linalg.norm(xref))
+    out = {"gpu_ms_100_iterations": ms, "rel_l2_vs_reference_sirt": rel,
+           "config": "SIRT, ray-driven pair, 256x256, 304 angles, 100 iterations, x0 = 1"}
+    if cpu:
+        from oracle.oracle import RefLib, radon_angles
+        R = RefLib()
+        ang = radon_angles(deg)
+        img = xref.astype(np.float32)
+        t0 = time.perf_counter()
+        y = R.radon("rd", 0, img, ang)
+        t1 = time.perf_counter()
+        R.radon("rd", 1, y, ang)
+        t2 = time.perf_counter()
+        ref_s = 100 * (2 * (t1 - t0) + (t2 - t1))
+        out["reference_s_100_iterations"] = ref_s
+        out["reference_sample"] = ("reference radon_rd (oracle/_ref) one forward and one adjoint timed on 1 core, "
+                                   "x 100 iterations of 2 forward + 1 adjoint")
+        out["speedup"] = ref_s / (ms * 1e-3)
+    del solver
+    return out
+
+
+def c2_core(dev):
+    """C2: MLEM and SPS (no penalty) with the distance-driven pair, 512 x 512
+    phantom (seed 1) scaled to mu in [0, 0.02] and centred in 768 bins, 720
+    angles on [0, 180), 50 iterations from x0 = 1: MLEM on the noiseless sinogram
+    (on the noisy one the reference MLEM diverges), SPS on -log(max(counts,1)/1e4),
+    counts ~ Poisson(1e4 exp(-A mu)).  The sinograms and the reference's own 50-
+    iteration results and wall times come from tests/golden/solver_c2_<algo>.npz
+    (sir.em / sir.sps over the compiled reference projector, one core); the
+    GPU time is the fused solver's 50 iterations under CUDA events."""
+    import torch
+    from iterative_tomographic_reconstruction_algorithms_b200 import class_projectors_radon as cpr
+    from iterative_tomographic_reconstruction_algorithms_b200.solvers import Solver
+    out = {"config": "MLEM / SPS, distance-driven pair, 512^2 phantom in 768 bins, 720 angles, 50 iterations"}
+    deg = np.linspace(0, 180, 720, endpoint=False)
+    tp = cpr.projectors(768, deg, oper="dd")
+    for algo in ("em", "sps"):
+        f = ROOT / "tests" / "golden" / f"solver_c2_{algo}.npz"
+        if not f.exists():
+            out[algo] = {"skipped": "fixture absent"}
+            continue
+        g = np.load(f)
+        solver = Solver(tp, algo, g["b"])
+        x0 = torch.ones((1, 768, 768), device=dev)
+        solver.run(x0, 1)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        x, _ = solver.run(x0, 50)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        xh, xr = x[0].cpu().numpy().astype(np.float64), g["x50"].astype(np.float64)
+        out[algo] = {"gpu_ms_50_iterations": ms, "rel_l2_vs_reference": float(np.linalg.norm(xh - xr) / np.linalg.norm(xr)),
+                     "reference_s_50_iterations": float(g["ref_seconds"][0]),
+                     "reference_host": "the fixture's build container, 1 core",
+                     "speedup": float(g["ref_seconds"][0]) / (ms * 1e-3)}
+        del solver
+    return out
+
+
+def run_blocks(args, dev):
+    """The configurations beside the headline, each measured in this process
+    (device time by CUDA events): C1 SIRT + rd, C2 MLEM / SPS + dd, C3 ADMM-TV +
+    gridding (with the gridding roofline), C4 batched uneven SIRT, C5 learned
+    warm start.  A block that fails records its error and the others still run."""
+    import torch
+    blocks = {}
+    jobs = [("c1_sirt_rd", lambda: c1_core(dev)),
+            ("c2_mlem_sps_dd", lambda: c2_core(dev)),
+            ("c3_admm_tv_grid", lambda: admm_core(3, 1, dev, cpu_baseline=False)),
+            ("c4_batched_sirt", lambda: batch_core(args.block_slices, args.block_iters, 1, 1, 0, 1, dev)),
+            ("c5_warm_start", lambda: warmstart_core(args.train_pairs, args.train_steps, args.eval_slices,
+                                                     args.lam, dev))]
+    for name, fn in jobs:
+        t0 = time.perf_counter()
+        try:
+            blocks[name] = fn()
+        except Exception as e:  # noqa: BLE001 -- a block's failure is recorded, not fatal
+            blocks[name] = {"error": f"{type(e).__name__}: {e}"}
+        blocks[name]["seconds"] = time.perf_counter() - t0
+        torch.cuda.empty_cache()
+    return blocks
 
 
 # gathered operand bytes per pixel x angle update of each projector (its reference
@@ -621,10 +835,11 @@ def main():
     peaks_file = ROOT / "MEASURED_PEAKS.json"
     hbm_peak = json.loads(peaks_file.read_text())["hbm_gbs"] if peaks_file.exists() else 6650.0
 
+    blocks = run_blocks(args, dev) if (world == 1 and not args.no_blocks) else None
     if rank == 0:
         cpu = None
         if world == 1:
-            g, dt, desc = cpu_reference_gups(n, na, 4, 1)
+            g, dt, desc = cpu_reference_gups(n, na, args.cpu_sample_angles or 16, 1)
             cpu = {"value": g, "unit": UNIT, "cores": 1, "kind": "reference", "sample": desc}
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -646,6 +861,8 @@ def main():
             "clocks": clk.summary(),
             "cpu_baseline": cpu,
         }
+        if blocks is not None:
+            line["blocks"] = blocks
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
