@@ -347,8 +347,9 @@ def warmstart_core(train_pairs, train_steps, eval_slices, lam, dev, oracle_slice
     trained on them with the tensor-core kernels, then on held-out seeds 100000 + i the
     GPU time plain SIRT needs for its 300 iterations against the time the warm start
     (2 iterations + network + fallback check + SIRT) needs to reach the same data
-    residual.  The final data residuals of ``oracle_slices`` held-out slices are also
-    computed with the FP64 oracle.  Metric: warm / plain time (lower is better)."""
+    residual (summed over the held-out slices).  For ``oracle_slices`` of them the
+    final data residuals of both runs are computed again with the FP64 oracle's
+    projector beside the GPU's.  Metric: warm / plain time (lower is better)."""
     import torch
     from iterative_tomographic_reconstruction_algorithms_b200 import nn, warmstart as ws
     pb = ws.Problem()
@@ -366,8 +367,14 @@ def warmstart_core(train_pairs, train_steps, eval_slices, lam, dev, oracle_slice
     r = ws.time_to_residual(net, pb, [100000 + i for i in range(eval_slices)])
     k = min(oracle_slices, eval_slices)
     bh = r["b"][:k].cpu().numpy()
-    res_p = oracle_residuals(r["x_plain"][:k].cpu().numpy(), bh, pb.na)
-    res_w = oracle_residuals(r["x_warm"][:k].cpu().numpy(), bh, pb.na)
+    tp = r["tp"]
+    fp64 = {"slices": k}
+    for name in ("plain", "warm"):
+        x = r[f"x_{name}"][:k]
+        gpu = ((tp.A(x).double() - r["b"][:k].double()) ** 2).sum(dim=(1, 2)).cpu().numpy()
+        orc = np.array(oracle_residuals(x.cpu().numpy(), bh, pb.na))
+        fp64[name] = {"gpu": gpu.tolist(), "oracle": orc.tolist(),
+                      "max_rel_diff": float(np.max(np.abs(gpu - orc) / orc))}
     out = {"value": r["ratio"], "unit": "ratio (warm / plain GPU time)", "higher_is_better": False,
            "config": {"workload": "512^2 phantom in 768 bins, 180 angles, Poisson I0=5e3, dd pair, SIRT from 0; "
                                   "U-Net 4 levels x 32 channels, BF16 weights/activations, FP32 accumulation",
@@ -378,7 +385,7 @@ def warmstart_core(train_pairs, train_steps, eval_slices, lam, dev, oracle_slice
            "residual_warm": r["residual_warm"], "image_rel_err_plain": r["err_plain"],
            "image_rel_err_warm": r["err_warm"], "image_rel_err_start": r["err_start"],
            "fallback_slices": r["fallback_slices"],
-           "fp64_oracle_residual": {"slices": k, "plain": res_p, "warm": res_w},
+           "fp64_oracle_residual": fp64,
            "pairs_s": t_pairs, "train_s": t_train, "loss_first_last": [hist[0], hist[-1]] if hist else None}
     del r, net
     torch.cuda.empty_cache()
@@ -465,6 +472,8 @@ def admm_core(steps, warmup, dev, cpu_baseline=True):
     # ceil(lconv)^2 window of complex64 taps (8 B and 8 flops a tap), plus the 2-D FFT
     # (5 pdim^2 log2(pdim^2) flops); peaks: L1 16-byte loads and FP32 FMA, measured now
     pk = onchip_peaks()
+    peaks_file = ROOT / "MEASURED_PEAKS.json"
+    hbm_peak = json.loads(peaks_file.read_text())["hbm_gbs"] if peaks_file.exists() else 6650.0
     from iterative_tomographic_reconstruction_algorithms_b200.gridrec_lut import grid_size
     pdim = grid_size(n, 2.0)
     roof = {}
@@ -473,8 +482,14 @@ def admm_core(steps, warmup, dev, cpu_baseline=True):
         flops = 8.0 * taps + 5.0 * pdim * pdim * math.log2(pdim * pdim)
         gb = 8.0 * taps / (t_ms * 1e-3) / 1e9
         tf = flops / (t_ms * 1e-3) / 1e12
+        # HBM passes over the complex64 Fourier grid: written once (fill / gather), two
+        # read+write passes of the 2-D FFT, read once (gather / deapodise), plus the
+        # na x pdim polar rows written and read once
+        hbm = 8.0 * (6.0 * pdim * pdim + 2.0 * na * pdim)
+        hb = hbm / (t_ms * 1e-3) / 1e9
         roof[name] = {"ms": t_ms, "window": math.ceil(lconv), "gathered_gbs": gb, "frac_of_l1": gb / pk["l1_gbs"],
-                      "tflops": tf, "frac_of_fp32": tf / pk["fp32_tflops"]}
+                      "tflops": tf, "frac_of_fp32": tf / pk["fp32_tflops"],
+                      "hbm_bytes_passes": hbm, "hbm_gbs": hb, "frac_of_hbm": hb / hbm_peak}
     out = {
         "metric": "ADMM-TV outer iterations per second (gridding pair, 5 inner CG iterations)",
         "value": 1e3 / ms, "unit": "iterations/s", "n_gpus": 1, "steps": steps, "warmup": warmup,

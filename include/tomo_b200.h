@@ -71,7 +71,12 @@ typedef struct tomo_geom {
   const float *grid_lut;
   int grid_lut_len;
   const float *grid_deapod;
-  int grid_mode;        /* 0 = compat (reference arithmetic), 1 = matched adjoint */
+  int grid_mode;        /* 0 = compat: the reference's arithmetic in both directions
+                         *     (gridrec_v4_forwproj.c, gridrec_v4_backproj.c);
+                         * 1 = matched: the forward unchanged, the adjoint its
+                         *     exact transpose (the forward's kernel width, the
+                         *     transpose of the crop, consistent Hermitian halves);
+                         *     no reference counterpart */
 } tomo_geom;
 
 /* Last error message of the calling thread ("" if none).  Returns TOMO_OK. */

@@ -68,6 +68,15 @@ int tomo_nn_relu_bwd(const void *Y, void *dY, size_t n, void *stream);
 int tomo_nn_adam(float *p, const float *g, float *m, float *v, size_t n, float lr, float beta1, float beta2,
                  float eps, int step, void *stream);
 
+/* How many times the tensor-core kernels poll a pipeline barrier (the wait
+ * for the MMAs that read a shared-memory stage before it is refilled) before
+ * they give up: spins >= 0 sets the limit for later launches in this process
+ * (0: give up at once, which only serves to exercise the give-up path), spins
+ * < 0 restores the default of 2^22.  A kernel that gives up sets bit 0 of the
+ * status word, stores nothing, and before freeing its tensor memory waits for
+ * its last committed MMAs with the long default limit whatever this setting. */
+int tomo_nn_set_wait_limit(int spins);
+
 /* Reads and clears the device status word of the current device (bit 0: a
  * tensor-core wait gave up); synchronises the device. */
 int tomo_nn_status(unsigned *flags);

@@ -8,9 +8,11 @@ forward launch -- no tape of the projector's internals, no float atomics, so
 gradients are deterministic.  For the radon and B-spline pairs ``A^T`` is the
 exact transpose of ``A`` (as in the reference C, where both directions walk the
 same indices and weights), so these gradients are exact.  The gridding pair
-reproduces the reference's asymmetric forward/adjoint (different kernel
-widths, edge-replicated projections): there the backward is the reference's
-adjoint, not the transpose, and is flagged with ``exact_gradient = False``.
+by default reproduces the reference's asymmetric forward/adjoint (different
+kernel widths, edge-replicated projections): there the backward is the
+reference's adjoint, not the transpose, and is flagged with
+``exact_gradient = False``; built with ``adjoint="matched"`` its adjoint is the
+exact transpose and the flag is True.
 
 ``sirt_unrolled`` runs SIRT iterations (algorithms/art.py:211-237 of the
 reference: ``x <- x + C A^T(R (b - A x))``, ``R = 1/A1``, ``C = 1/A^T 1``,
@@ -61,7 +63,8 @@ class Projector(torch.nn.Module):
         self.tp = tp
         self.n = int(getattr(tp, "npix", 0) or getattr(tp, "n"))
         self.na = int(tp.nang)
-        self.exact_gradient = tp.__class__.__module__.split(".")[-1] != "class_projectors_grid"
+        is_grid = tp.__class__.__module__.split(".")[-1] == "class_projectors_grid"
+        self.exact_gradient = (not is_grid) or getattr(tp, "adjoint", "compat") == "matched"
 
     def _plan(self, x, batched_ndim):
         if not (isinstance(x, torch.Tensor) and x.is_cuda and x.dtype == torch.float32):

@@ -14,6 +14,12 @@ edge-replicates the projections), run on the GPU (libtomo_b200.so: hand-written
 interpolation, deapodisation and 1-D FFTs, cuFFT for the 2-D transform).
 ``fbp`` is the adjoint with the configured reconstruction filter (ramp by
 default), as in the reference.
+
+``adjoint="matched"`` (a keyword beyond the reference's) makes ``At`` the exact
+transpose of ``A`` instead (same kernel width as the forward, zero-padded
+projections, consistent Hermitian halves), so the pair passes the adjoint
+dot-product test and its gradient is exact; ``A`` and ``fbp`` are unchanged.
+On band-limited images supported in the inscribed circle both adjoints agree.
 """
 from __future__ import annotations
 
@@ -32,7 +38,7 @@ class projectors:
     """Gridding projector pair (PSWF or Kaiser-Bessel interpolation)."""
 
     def __init__(self, npix, angles, ctr=0.0, kernel="pswf", oversampl=2.0, interp="nn",
-                 radon_degree=0, W=7.0, errs=1e-3, filt=None, args=None, verbose=True):
+                 radon_degree=0, W=7.0, errs=1e-3, filt=None, args=None, verbose=True, adjoint="compat"):
         if args is not None:
             kernel = args.kernel
             oversampl = args.oversampl
@@ -55,6 +61,9 @@ class projectors:
         self.param_filt = param_filt.astype(myfloat)
         self.nang = len(angles)
         self.npix = int(npix)
+        if adjoint not in ("compat", "matched"):
+            raise ValueError("adjoint must be 'compat' or 'matched'")
+        self.adjoint = adjoint
         self._plans = {}
         if verbose:
             print("\nSetting of the regridding projectors:")
@@ -73,7 +82,8 @@ class projectors:
         if p is None:
             param = self.param_nofilt if which == "nofilt" else self.param_filt
             kw = dict(grid_param=param, grid_lut=self.lut, grid_lut_len=len(self.lut),
-                      grid_deapod=self.deapod)
+                      grid_deapod=self.deapod,
+                      grid_mode=1 if (self.adjoint == "matched" and which == "nofilt") else 0)
             if device is not None:
                 import torch
                 with torch.cuda.device(device):

@@ -29,6 +29,16 @@
 // negative bound (samples near the grid edge at angles near 180 degrees)
 // turns its loop into a no-op: such samples contribute nothing, here too.
 //
+// Matched adjoint (grid_mode 1): the exact transpose of the forward above,
+// so that <A x, y> = <x, A^T y>.  The forward is y = Re(P x) with P complex-
+// linear, hence A^T y = Re(P^H y): the projection zero-padded (the adjoint of
+// the crop) and scaled by 1/pdim; its 1-D DFT with sign +1 (for a real row,
+// the conjugate of the sign -1 transform); per polar sample the values the
+// forward's two gathers took, f_w rho[pdim - w] for the window and
+// conj(f_w) rho[w] for its mirror (f the forward's centring filter); the
+// forward's window (lconv 2*7/pi, same LUT, same skip rules) gathered back into
+// H; the 2-D DFT with sign -1; the forward's deapodisation, crop and flip.
+//
 // Only the 2-D transform uses cuFFT; the per-projection 1-D transforms are a
 // mixed-radix Stockham FFT in shared memory (radix 4/2/3/5/7 and generic odd
 // primes; Govindaraju et al., SC'08 formulation).
@@ -51,6 +61,7 @@ struct GridState {
   float h_f = 0, tbl_f = 0;  // forward: lconv/2 and table spacing
   float h_b = 0, tbl_b = 0;  // adjoint
   float inv_pdim = 0;        // float(1.0/pdim)
+  bool matched = false;      // grid_mode 1: the adjoint is the forward's exact transpose
   int nfac = 0;
   int fac[32] = {0};
   float *lut = nullptr, *deapod = nullptr;
@@ -300,6 +311,41 @@ __global__ void __launch_bounds__(kFftThreads) grid_fft_adj_kernel(
       r.w = 0.0f;
     }
     dst[j] = r;
+  }
+}
+
+// Matched adjoint step 1: rho = the projection zero-padded to pdim and scaled
+// by 1/pdim, o = its sign -1 DFT; rho^ = conj(o) is the sign +1 DFT, and by
+// the Hermitian symmetry of a real row conj(o[pdim - w]) = o[w].  cd[w] =
+// {f_w rho^[pdim - w] (window), conj(f_w) rho^[w] (mirror, w != 0)}.
+__global__ void __launch_bounds__(kFftThreads) grid_fft_adj_matched_kernel(
+    const float *__restrict__ sino, float4 *__restrict__ cd, const float2 *__restrict__ tw,
+    const float2 *__restrict__ filt, FftConst c, int npix, int padleft, int pdim_h, float scale) {
+  extern __shared__ float2 sm[];
+  float2 *a = sm, *b = sm + c.n;
+  const size_t row = blockIdx.x;
+  const float *src = sino + row * npix;
+  for (int i = threadIdx.x; i < c.n; i += blockDim.x) {
+    const int k = i - padleft;
+    a[i] = make_float2(k >= 0 && k < npix ? __fmul_rn(scale, src[k]) : 0.0f, 0.0f);
+  }
+  __syncthreads();
+  const float2 *o = stockham(a, b, c, tw);
+  float4 *dst = cd + row * pdim_h;
+  for (int w = threadIdx.x; w < pdim_h; w += blockDim.x) {
+    const float2 f = filt[w], d = o[w];                       // rho^[pdim - w] = o[w]
+    float4 r;
+    r.x = __fmaf_rn(f.x, d.x, -__fmul_rn(f.y, d.y));
+    r.y = __fmaf_rn(f.x, d.y, __fmul_rn(f.y, d.x));
+    if (w != 0) {
+      const float2 m = o[c.n - w];                            // rho^[w] = o[pdim - w]
+      r.z = __fmaf_rn(f.x, m.x, __fmul_rn(f.y, m.y));        // conj(f) m
+      r.w = __fmaf_rn(f.x, m.y, -__fmul_rn(f.y, m.x));
+    } else {
+      r.z = 0.0f;
+      r.w = 0.0f;
+    }
+    dst[w] = r;
   }
 }
 
@@ -629,7 +675,9 @@ int grid_setup(Plan &p) {
   g->radon_degree = (int)prm[7];
   g->lut_len = G.grid_lut_len;
   if (flag_filter != 0) return fail(TOMO_EINVAL, "grid: only the built-in filter (param[2] == 0) is provided");
-  if (G.grid_mode != 0) return fail(TOMO_EINVAL, "grid: only grid_mode 0 (the reference's arithmetic) is provided");
+  if (G.grid_mode != 0 && G.grid_mode != 1)
+    return fail(TOMO_EINVAL, "grid: grid_mode must be 0 (the reference's arithmetic) or 1 (matched adjoint)");
+  g->matched = G.grid_mode == 1;
   if (g->ltbl + 2 > g->lut_len) return fail(TOMO_EINVAL, "grid: param[5] exceeds the lut length");
   // pdim: gridrec_v4_forwproj.c:128-130
   int pdim = (int)(std::pow(2, (int)std::ceil(std::log10((double)npix) / std::log10(2.0))) * oversampl);
@@ -722,6 +770,7 @@ int grid_setup(Plan &p) {
   const int smem = (int)(2 * sizeof(float2) * pdim);
   TOMO_CUDA(cudaFuncSetAttribute(grid_fft_fwd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
   TOMO_CUDA(cudaFuncSetAttribute(grid_fft_adj_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  TOMO_CUDA(cudaFuncSetAttribute(grid_fft_adj_matched_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
   p.fwd_warps = (size_t)nz * na * (kFftThreads / 32);
   return TOMO_OK;
 }
@@ -756,17 +805,23 @@ int grid_adjoint(Plan &p, const float *d_sino, float *d_img, cudaStream_t s, con
   GridState &g = *(GridState *)p.ext;
   const int npix = p.g.n, na = p.g.na, nz = p.g.nz, pdim = g.pdim;
   const int smem = (int)(2 * sizeof(float2) * pdim);
-  grid_fft_adj_kernel<<<na * nz, kFftThreads, smem, s>>>(d_sino, g.cd, g.tw, g.filt_b, fft_const(g), npix,
-                                                         g.padleft, g.pdim_h, g.radon_degree,
-                                                         (float)(1.0 / pdim));
-  GatherArgs ga{g.cd, g.H, g.sc4, g.sorted, g.lut, pdim, g.pdim_h, na, g.interp, 0, g.h_b, g.tbl_b};
+  if (g.matched)
+    grid_fft_adj_matched_kernel<<<na * nz, kFftThreads, smem, s>>>(d_sino, g.cd, g.tw, g.filt_f, fft_const(g),
+                                                                   npix, g.padleft, g.pdim_h, g.inv_pdim);
+  else
+    grid_fft_adj_kernel<<<na * nz, kFftThreads, smem, s>>>(d_sino, g.cd, g.tw, g.filt_b, fft_const(g), npix,
+                                                           g.padleft, g.pdim_h, g.radon_degree,
+                                                           (float)(1.0 / pdim));
+  GatherArgs ga{g.cd, g.H, g.sc4, g.sorted, g.lut, pdim, g.pdim_h, na, g.interp, 0,
+                g.matched ? g.h_f : g.h_b, g.matched ? g.tbl_f : g.tbl_b};
   ga.centre = std::min(kGatherCentre, g.pdim_h - 1);
   const int side = 2 * ga.centre + 1;
   grid_gather_centre_kernel<<<dim3((side * side + 3) / 4, nz), 128, 0, s>>>(ga);
   dim3 gb(128), gg((pdim + 127) / 128, pdim, nz);
   grid_gather_kernel<<<gg, gb, 0, s>>>(ga);
   if (cufftSetStream(g.fft2, s) != CUFFT_SUCCESS ||
-      cufftExecC2C(g.fft2, (cufftComplex *)g.H, (cufftComplex *)g.H, CUFFT_INVERSE) != CUFFT_SUCCESS)
+      cufftExecC2C(g.fft2, (cufftComplex *)g.H, (cufftComplex *)g.H, g.matched ? CUFFT_FORWARD : CUFFT_INVERSE) !=
+          CUFFT_SUCCESS)
     return fail(TOMO_ECUDA, "grid: 2-D FFT failed");
   dim3 eb(32, 8), eg((npix + 31) / 32, (npix + 7) / 8, nz);
   grid_extract_kernel<<<eg, eb, 0, s>>>(g.H, d_img, g.deapod, pdim, g.pdim_h, g.padleft, npix, ep);

@@ -17,9 +17,10 @@
 // rows x 16 B between K groups), by 16-byte cp.async copies (zero-filled
 // outside the matrix), double-buffered: the copies of K block k+1 overlap
 // the MMAs of block k.  One thread issues the MMAs and commits them to a
-// per-stage mbarrier; every wait on it is bounded, and a wait that gives up
-// records an error in the status word, waits (bounded) for the MMAs in flight,
-// frees the TMEM and returns.  The epilogue reads TMEM with tcgen05.ld
+// per-stage mbarrier; every wait on it is bounded (the pipeline waits by a
+// limit the caller may lower, tomo_nn_set_wait_limit), and a wait that gives
+// up records an error in the status word, waits (with a long limit) for the
+// last committed MMAs, frees the TMEM and returns without storing.  The epilogue reads TMEM with tcgen05.ld
 // (warp w owns accumulator rows 32w..32w+31), applies bias and ReLU and
 // stores FP32 or BF16.  With ksplit > 1 the K range is split over gridDim.z
 // and each slice writes a partial FP32 tile, summed afterwards in a fixed
@@ -34,7 +35,9 @@ namespace tomo_nn {
 namespace {
 
 constexpr int BM = 128, BK = 64, kThreads = 128;
-constexpr int kWaitSpins = 1 << 22;
+// Drain limit: the wait for the last committed MMAs before the TMEM is freed
+// keeps this long limit whatever the pipeline waits' limit (GemmArgs::spins).
+constexpr int kDrainSpins = 1 << 22;
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
   return (uint32_t)__cvta_generic_to_shared(p);
@@ -64,9 +67,10 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
-// Bounded wait for phase `parity` of the barrier; false if it gave up.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
-  for (int i = 0; i < kWaitSpins; ++i)
+// Bounded wait for phase `parity` of the barrier: at most `spins` polls;
+// false if it gave up (at once when spins is 0).
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int spins) {
+  for (int i = 0; i < spins; ++i)
     if (mbar_try_wait(bar, parity)) return true;
   return false;
 }
@@ -186,6 +190,7 @@ __global__ void __launch_bounds__(kThreads) gemm_tc_kernel(GemmArgs g) {
   const uint32_t tmem = *tmem_slot;
   const uint32_t idesc = instr_desc(BN);
   bool ok = true;
+  int last = -1;  // last K block whose MMAs were committed (block-uniform)
 
   if (nkb > 0) load_stage<BN>(g, m0, n0, kb0, smem_u32(sA[0]), smem_u32(sB[0]));
   cp_async_commit();
@@ -194,7 +199,7 @@ __global__ void __launch_bounds__(kThreads) gemm_tc_kernel(GemmArgs g) {
     if (it + 1 < nkb) {
       // the stage about to be refilled was read by the MMAs of block it-1
       if (it >= 1) {
-        const bool w = mbar_wait(smem_u32(&bars[s ^ 1]), ((it - 1) >> 1) & 1);
+        const bool w = mbar_wait(smem_u32(&bars[s ^ 1]), ((it - 1) >> 1) & 1, g.spins);
         ok = __syncthreads_and(w) != 0;  // block-uniform
         if (!ok) break;
       }
@@ -218,14 +223,17 @@ __global__ void __launch_bounds__(kThreads) gemm_tc_kernel(GemmArgs g) {
       mma_commit(smem_u32(&bars[s]));
     }
     __syncwarp();
+    last = it;
   }
   cp_async_wait<0>();
-  // the last commit covers every MMA issued before it (on the error path:
-  // one more bounded wait for the MMAs in flight before the TMEM is freed)
-  if (nkb > 0) {
-    const bool done = mbar_wait(smem_u32(&bars[(nkb - 1) & 1]), ((nkb - 1) >> 1) & 1);
+  // The last commit covers every MMA issued before it; it is also where the
+  // error path (a pipeline wait that gave up, `last` = the block before it)
+  // waits, with the long drain limit, before the TMEM is freed.  If even that
+  // gives up, the TMEM is still freed: the status word says the output and the
+  // kernel are not to be trusted.
+  if (last >= 0) {
+    const bool done = mbar_wait(smem_u32(&bars[last & 1]), (last >> 1) & 1, kDrainSpins);
     ok = __syncthreads_and(ok && done) != 0;
-    if (!ok) mbar_wait(smem_u32(&bars[(nkb - 1) & 1]), ((nkb - 1) >> 1) & 1);
   }
   if (!ok && tid == 0 && g.status) atomicOr(g.status, 1);
   tc_fence_after();

@@ -29,7 +29,9 @@ struct GemmArgs {
   int relu = 0;
   int ksplit = 1;
   unsigned *status = nullptr;        // bit 0 set if an MMA wait gave up
+  int spins = 1 << 22;               // polls of a pipeline wait before it gives up
 };
+
 
 int gemm_launch(const GemmArgs &g, cudaStream_t s);
 

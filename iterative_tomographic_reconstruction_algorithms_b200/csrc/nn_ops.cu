@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <mutex>
 
 #include "nn_internal.cuh"
@@ -13,6 +14,7 @@ namespace tomo_nn {
 namespace {
 
 __device__ unsigned g_status;  // bit 0: a tensor-core wait gave up
+std::atomic<int> g_wait_spins{1 << 22};
 
 unsigned *status_ptr() {
   static std::mutex mu;
@@ -147,6 +149,7 @@ int tomo_nn_gemm(const void *A, int lda, const void *B, int ldb, int M, int N, i
   g.bias = bias;
   g.relu = relu;
   g.status = status_ptr();
+  g.spins = g_wait_spins.load();
   return gemm_launch(g, (cudaStream_t)stream);
 }
 
@@ -170,6 +173,7 @@ int tomo_nn_conv3x3(const void *X, int batch, int H, int W, int Cin, const void 
   g.bias = bias;
   g.relu = relu;
   g.status = status_ptr();
+  g.spins = g_wait_spins.load();
   return gemm_launch(g, (cudaStream_t)stream);
 }
 
@@ -212,6 +216,7 @@ int tomo_nn_wgrad(const void *X, const void *dY, int batch, int H, int W, int Ci
   g.ldc = Cout;
   g.ksplit = S;
   g.status = status_ptr();
+  g.spins = g_wait_spins.load();
   if (P > 0x7fffffffLL) return NN_EINVAL;
   int rc = gemm_launch(g, s);
   if (rc) return rc;
@@ -243,6 +248,11 @@ int tomo_nn_adam(float *p, const float *g, float *m, float *v, size_t n, float l
   adam_kernel<<<(unsigned)std::min<size_t>((n + 255) / 256, 148 * 16), 256, 0, (cudaStream_t)stream>>>(
       p, g, m, v, n, lr, beta1, beta2, eps, c1, c2);
   return cudaGetLastError() == cudaSuccess ? NN_OK : NN_ECUDA;
+}
+
+int tomo_nn_set_wait_limit(int spins) {
+  tomo_nn::g_wait_spins.store(spins < 0 ? (1 << 22) : spins);
+  return NN_OK;
 }
 
 int tomo_nn_status(unsigned *flags) {

@@ -441,6 +441,14 @@ __device__ __forceinline__ void dd_fwd_crossings(const double2 *__restrict__ SL,
       // lines on which the crossing lies within [P_0, P_n]: q in [-nh - B - 2, n - nh - B + 2]
       int ia, ib;
       dd_line_range(-(double)nh - B - 2.0, (double)(n - nh) - B + 2.0, (double)k, n, nh, ia, ib);
+      // and on which delta can be nonzero: a float q with |q| >= 2^e is a
+      // multiple of both binades' spacings (2^(e-24), 2^(e-23)), so then both
+      // roundings are exact and the width is 1: only |y k| < 2^e matters
+      const double ymax = ldexp(1.0, e) * (1.0 + 1e-6) / fabs((double)k) + 1.0;
+      if (ymax < (double)n) {
+        ia = max(ia, (int)floor((double)nh - 0.5 - ymax));
+        ib = min(ib, (int)ceil((double)nh - 0.5 + ymax));
+      }
       double a[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll 1
       for (int i = ia + lane; i <= ib; i += 32) {

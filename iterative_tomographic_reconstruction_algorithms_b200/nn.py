@@ -61,6 +61,13 @@ def _p(t):
     return ctypes.c_void_p(t.data_ptr()) if t is not None else None
 
 
+def set_wait_limit(spins: int) -> None:
+    """Polls of a tensor-core pipeline wait before it gives up (tomo_nn.h:
+    tomo_nn_set_wait_limit); a negative value restores the default."""
+    lib.tomo_nn_set_wait_limit.argtypes = [ctypes.c_int]
+    _check(lib.tomo_nn_set_wait_limit(int(spins)), "tomo_nn_set_wait_limit")
+
+
 def check_status():
     """Raises if a tensor-core wait gave up in any kernel since the last check."""
     flags = ctypes.c_uint()

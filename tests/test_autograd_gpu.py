@@ -86,6 +86,33 @@ def test_gridding_gradient_is_flagged_inexact(cuda):
     from iterative_tomographic_reconstruction_algorithms_b200.autograd import Projector
     tp = cpg.projectors(64, np.linspace(0, 180, 48, endpoint=False), verbose=False)
     assert not Projector(tp).exact_gradient
+    tpm = cpg.projectors(64, np.linspace(0, 180, 48, endpoint=False), verbose=False, adjoint="matched")
+    assert Projector(tpm).exact_gradient
+
+
+def test_matched_gridding_gradient_matches_finite_differences(cuda):
+    """With the matched adjoint the backward of A is A^T exactly: the gradient
+    of 0.5 |A x - b|^2 along a random direction equals the central difference."""
+    torch = cuda
+    from iterative_tomographic_reconstruction_algorithms_b200 import class_projectors_grid as cpg
+    from iterative_tomographic_reconstruction_algorithms_b200.autograd import Projector
+    n, na = 64, 60
+    tp = cpg.projectors(n, np.linspace(0, 180, na, endpoint=False), kernel="kb", W=6.0, interp="lin",
+                        verbose=False, adjoint="matched")
+    op = Projector(tp)
+    g = torch.Generator().manual_seed(3)
+    x = torch.randn((n, n), generator=g).cuda().requires_grad_(True)
+    b = torch.randn((na, n), generator=g).cuda()
+    d = torch.randn((n, n), generator=g).cuda()
+    loss = 0.5 * ((op(x) - b) ** 2).sum(dtype=torch.float64)
+    loss.backward()
+    gd = float((x.grad.double() * d.double()).sum())
+    eps = 1e-2
+    with torch.no_grad():
+        lp = 0.5 * ((op(x + eps * d) - b).double() ** 2).sum()
+        lm = 0.5 * ((op(x - eps * d) - b).double() ** 2).sum()
+    fd = float((lp - lm) / (2 * eps))
+    assert abs(gd - fd) <= 1e-4 * abs(fd)
 
 
 def test_unrolled_sirt_matches_fused_solver_and_checkpointing(cuda):

@@ -5,7 +5,9 @@ The reference's own golden vector for this path is data/shepp_logan_pix0256.tif
 and its grid-PSWF sinogram data/shepp_logan_pix0256_ang0304_sino.tif (stored in
 tests/golden/grid_golden.npz as "sl/*").  The reference gridding pair is not an
 adjoint pair (its forward fixes the kernel width at 2*7/pi, its adjoint
-edge-replicates the projections), so there is no dot-product test here.
+edge-replicates the projections), so the compat mode has no dot-product test;
+the matched mode (adjoint="matched": the forward's exact transpose) has one,
+on N(0,1) data, to 1e-5.
 """
 from __future__ import annotations
 
@@ -116,3 +118,51 @@ def test_dropin_entry_points_overwrite(cuda, grid_golden):
            tp.lut.ctypes.data_as(fp), tp.deapod.ctypes.data_as(fp), None, rec.ctypes.data_as(fp), None)
     assert rc == 0, _lib.last_error()
     assert rel_l2(rec, grid_golden[f"{case}/adj"]) <= TOL
+
+
+MATCHED_CASES = [  # n, na, kernel, oversampling, interp, W
+    (64, 90, "pswf", 2.0, "nn", 7.0),
+    (96, 120, "kb", 2.0, "lin", 6.0),
+    (100, 75, "kb", 1.5, "lin", 6.6),      # pdim 192, not a power of two
+    (129, 61, "prolate", 2.0, "nn", 7.0),
+]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n,na,kernel,os_,interp,W", MATCHED_CASES)
+def test_matched_adjoint_passes_dot_test(cuda, n, na, kernel, os_, interp, W):
+    """<A x, y> = <x, A^T y> with float64 dot products, relative to |A x| |y|."""
+    from iterative_tomographic_reconstruction_algorithms_b200 import class_projectors_grid as cpg
+    tp = cpg.projectors(n, np.linspace(0, 180, na, endpoint=False), kernel=kernel, oversampl=os_,
+                        interp=interp, W=W, verbose=False, adjoint="matched")
+    rng = np.random.default_rng(7)
+    x = rng.standard_normal((n, n)).astype(np.float32)
+    y = rng.standard_normal((na, n)).astype(np.float32)
+    ax, aty = tp.A(x).astype(np.float64), tp.At(y).astype(np.float64)
+    lhs, rhs = float(np.sum(ax * y)), float(np.sum(x.astype(np.float64) * aty))
+    assert abs(lhs - rhs) / (np.linalg.norm(ax) * np.linalg.norm(y)) <= TOL
+    # A itself is the reference's forward in both modes
+    tpc = cpg.projectors(n, np.linspace(0, 180, na, endpoint=False), kernel=kernel, oversampl=os_,
+                         interp=interp, W=W, verbose=False)
+    assert np.array_equal(tp.A(x), tpc.A(x))
+
+
+@pytest.mark.gpu
+def test_matched_adjoint_agrees_with_reference_on_band_limited_in_circle_data(cuda, grid_golden):
+    """On a smooth image supported well inside the inscribed circle, and its
+    sinogram, the matched adjoint and the reference's (compat, same kernel
+    width for PSWF W = 7) differ only by what the reference does differently at
+    the edges of the padded projections and the grid: compared on the disk."""
+    from iterative_tomographic_reconstruction_algorithms_b200 import class_projectors_grid as cpg
+    n, na = 128, 180
+    deg = np.linspace(0, 180, na, endpoint=False)
+    kw = dict(kernel="pswf", oversampl=2.0, interp="lin", W=7.0, verbose=False)
+    tpm = cpg.projectors(n, deg, adjoint="matched", **kw)
+    tpc = cpg.projectors(n, deg, **kw)
+    c = (np.arange(n) - n / 2 + 0.5) / (n / 2)
+    X, Y = np.meshgrid(c, c)
+    img = np.exp(-((X - 0.1) ** 2 + (Y + 0.05) ** 2) / (2 * 0.15 ** 2)).astype(np.float32)
+    y = tpc.A(img)
+    disk = X ** 2 + Y ** 2 < 0.6 ** 2
+    am, ac = tpm.At(y), tpc.At(y)
+    assert rel_l2(am[disk], ac[disk]) <= 1e-2

@@ -127,3 +127,28 @@ def test_adam_matches_torch(cuda):
         opt.step()
         opt_ref.step()
     assert torch.allclose(p, q.detach(), rtol=1e-5, atol=1e-6)
+
+
+def test_pipeline_wait_gives_up_then_recovers(cuda):
+    """With the pipeline wait limit at 0, every GEMM of more than two K blocks
+    gives up at its first pipeline wait: it sets the status bit, stores nothing
+    and still waits (with the long drain limit) for its committed MMAs before
+    freeing its tensor memory, so nothing faults and nothing hangs.  The check
+    raises, the status clears, and with the default limit restored the same
+    GEMM is exact again."""
+    torch = cuda
+    from iterative_tomographic_reconstruction_algorithms_b200 import nn
+    A, B = _bf(torch, (256, 512), 3), _bf(torch, (64, 512), 4)   # K = 512: 8 blocks of 64
+    ref = A.double() @ B.double().T
+    nn.check_status()
+    try:
+        nn.set_wait_limit(0)
+        nn.gemm(A.cuda(), B.cuda())
+        with pytest.raises(RuntimeError, match="wait gave up"):
+            nn.check_status()
+    finally:
+        nn.set_wait_limit(-1)
+    nn.check_status()                      # cleared by the read above
+    out = nn.gemm(A.cuda(), B.cuda())
+    nn.check_status()
+    assert _relerr(torch, out, ref) < 1e-5
