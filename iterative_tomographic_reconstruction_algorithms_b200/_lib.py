@@ -156,7 +156,7 @@ class Plan:
     def sino_shape(self):
         return (self.nz, self.na, self.n)
 
-    def _run(self, x, fwd: bool):
+    def _run(self, x, fwd: bool, out=None):
         in_shape = self.image_shape if fwd else self.sino_shape
         out_shape = self.sino_shape if fwd else self.image_shape
         if isinstance(x, np.ndarray):
@@ -174,18 +174,24 @@ class Plan:
         if x.numel() != int(np.prod(in_shape)):
             raise ValueError(f"expected {in_shape} elements, got shape {tuple(x.shape)}")
         xin = x.contiguous()
-        out = torch.empty(out_shape, dtype=torch.float32, device=x.device)
+        if out is None:
+            out = torch.empty(out_shape, dtype=torch.float32, device=x.device)
+        elif not (isinstance(out, torch.Tensor) and out.is_cuda and out.dtype == torch.float32
+                  and out.is_contiguous() and out.numel() == int(np.prod(out_shape)) and out.device == x.device):
+            raise ValueError(f"out must be a contiguous CUDA float32 tensor of {out_shape} elements on x's device")
         stream = torch.cuda.current_stream(x.device).cuda_stream
         fn = lib.tomo_forward if fwd else lib.tomo_adjoint
         with self._lock:
             check(fn(self._h, xin.data_ptr(), out.data_ptr(), stream), "device projector call")
         return out
 
-    def forward(self, x):
-        return self._run(x, True)
+    def forward(self, x, out=None):
+        """A x; ``out`` (device path only) receives the result in place of a new tensor."""
+        return self._run(x, True, out)
 
-    def adjoint(self, y):
-        return self._run(y, False)
+    def adjoint(self, y, out=None):
+        """A^T y; ``out`` (device path only) receives the result in place of a new tensor."""
+        return self._run(y, False, out)
 
     def tuning(self) -> str:
         return plan_tuning(self)

@@ -8,59 +8,72 @@
 namespace tomo {
 namespace {
 
-constexpr int kSmemWords = 8192;  // 32 KiB of float4
 constexpr int kIters = 4096;
 
-// Shared-memory load bandwidth: conflict-free 16-byte loads, 8 in flight.
+// The loads of both probes are volatile inline PTX, so the compiler issues
+// every one of them (a plain loop over a periodic address pattern can be
+// folded, which once made a probe report nearly twice the bytes it moved).
+// Addresses are a base plus a constant offset per unrolled load, and each
+// load's value feeds one add, so the probes issue about two instructions per load and the
+// memory pipe, not the schedulers, is the limit.
+constexpr int kUnroll = 16;
+
+// Shared-memory load bandwidth: 16-byte loads, a warp request = 512
+// consecutive bytes (conflict-free), from a 32 KiB array.
 __global__ void __launch_bounds__(512) smem_probe(float *out, int salt) {
-  __shared__ float4 buf[kSmemWords / 4];
-  for (int i = threadIdx.x; i < kSmemWords / 4; i += blockDim.x)
-    buf[i] = make_float4(i + salt, i, i, i);
+  __shared__ __align__(16) float buf[8192];
+  for (int i = threadIdx.x; i < 8192; i += blockDim.x) buf[i] = (float)(i + salt);
   __syncthreads();
-  float4 acc[8];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t base = (uint32_t)__cvta_generic_to_shared(buf) + lane * 16;
+  uint32_t off = (warp * 3 * 512) & (32768 - 1) & ~(kUnroll * 512 - 1);
+  float acc = 0.0f;
+  for (int it = 0; it < kIters; it += kUnroll) {
+    const uint32_t a = base + off;
 #pragma unroll
-  for (int u = 0; u < 8; ++u) acc[u] = make_float4(0, 0, 0, 0);
-  const int mask = kSmemWords / 4 - 1;
-  int idx = threadIdx.x;
-  for (int it = 0; it < kIters; it += 8) {
-#pragma unroll
-    for (int u = 0; u < 8; ++u) {
-      float4 v = buf[(idx + u * 512) & mask];
-      acc[u].x += v.x; acc[u].y += v.y; acc[u].z += v.z; acc[u].w += v.w;
+    for (int u = 0; u < kUnroll; ++u) {
+      float x, y, z, w;
+      asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];"
+                   : "=f"(x), "=f"(y), "=f"(z), "=f"(w)
+                   : "r"(a + u * 512));
+      asm volatile("" ::"f"(y), "f"(z), "f"(w));  // the other lanes of the vector: no instruction
+      acc += x;
     }
-    idx += 64;
+    off = (off + kUnroll * 512) & (32768 - 1);
   }
-  float s = 0;
-#pragma unroll
-  for (int u = 0; u < 8; ++u) s += acc[u].x + acc[u].y + acc[u].z + acc[u].w;
-  if (s == 1234.5f) out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+  if (acc == 1234.5f) out[blockIdx.x * blockDim.x + threadIdx.x] = acc;
 }
 
-// L1 load bandwidth from a per-CTA 64 KiB window (L1-resident after the
-// first pass), with every warp request one aligned, fully used block of
-// memory: lane l of a warp reads word (base + l) for 4-byte loads (one 128-byte
-// line per request) and float4 (base + l) for 16-byte loads (four lines).
-// base steps by a multiple of the request size, so no request straddles lines.
-template <typename T>
-__global__ void __launch_bounds__(512) l1_probe(const T *__restrict__ src, float *out) {
-  constexpr int kWin = 65536 / sizeof(T);  // window in elements
-  const T *w = src + (size_t)(blockIdx.x % 8) * kWin;
+// L1 load bandwidth from a 32 KiB window that every CTA of an SM reads (so it
+// stays in L1 after the first pass).  VEC = 1: 4-byte loads, a warp request =
+// one 128-byte line; VEC = 4: 16-byte loads, four lines.  No request straddles
+// a line.
+template <int VEC>
+__global__ void __launch_bounds__(512) l1_probe(const float *__restrict__ src, float *out) {
+  constexpr int kReq = 32 * VEC * 4;  // bytes per warp request
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  float acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-  int base = warp * 32 * 8;
-  for (int it = 0; it < kIters; it += 8) {
+  const char *base = (const char *)src + lane * VEC * 4;
+  uint32_t off = (uint32_t)(warp * 3 * kReq) & (32768 - 1) & ~(uint32_t)(kUnroll * kReq - 1);
+  float acc = 0.0f;
+  for (int it = 0; it < kIters; it += kUnroll) {
+    const char *p = base + off;
 #pragma unroll
-    for (int u = 0; u < 8; ++u) {
-      const T v = __ldg(w + ((base + u * 32 + lane) & (kWin - 1)));
-      if constexpr (sizeof(T) == 16) acc[u] += v.x + v.y + v.z + v.w;
-      else acc[u] += v;
+    for (int u = 0; u < kUnroll; ++u) {
+      float x;
+      if constexpr (VEC == 1) {
+        asm volatile("ld.global.nc.f32 %0, [%1];" : "=f"(x) : "l"(p + u * kReq));
+      } else {
+        float y, z, w;
+        asm volatile("ld.global.nc.v4.f32 {%0, %1, %2, %3}, [%4];"
+                     : "=f"(x), "=f"(y), "=f"(z), "=f"(w)
+                     : "l"(p + u * kReq));
+        asm volatile("" ::"f"(y), "f"(z), "f"(w));  // the other lanes of the vector: no instruction
+      }
+      acc += x;
     }
-    base += 32 * 8 * 16 + 32;  // a multiple of 32 elements
+    off = (off + kUnroll * kReq) & (32768 - 1);
   }
-  float s = 0;
-#pragma unroll
-  for (int u = 0; u < 8; ++u) s += acc[u];
-  if (s == 1234.5f) out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+  if (acc == 1234.5f) out[blockIdx.x * blockDim.x + threadIdx.x] = acc;
 }
 
 // FP32 FMA rate: 8 independent dependency chains per thread.
@@ -108,16 +121,16 @@ extern "C" int tomo_measure_onchip_peaks2(double *smem_gbs, double *l1_4_gbs, do
   const int blocks = sms * 4, threads = 512;
   float *out = nullptr, *src = nullptr;
   TOMO_CUDA(cudaMalloc(&out, sizeof(float) * blocks * threads));
-  TOMO_CUDA(cudaMalloc(&src, 65536 * 8));
-  TOMO_CUDA(cudaMemset(src, 0, 65536 * 8));
+  TOMO_CUDA(cudaMalloc(&src, 32768));
+  TOMO_CUDA(cudaMemset(src, 0, 32768));
   float ms = 0;
   int rc = time_launch([&] { smem_probe<<<blocks, threads>>>(out, 1); }, 5, &ms);
   if (rc) return rc;
   if (smem_gbs) *smem_gbs = (double)blocks * threads * kIters * 16.0 / (ms * 1e-3) / 1e9;
-  rc = time_launch([&] { l1_probe<float><<<blocks, threads>>>(src, out); }, 5, &ms);
+  rc = time_launch([&] { l1_probe<1><<<blocks, threads>>>(src, out); }, 5, &ms);
   if (rc) return rc;
   if (l1_4_gbs) *l1_4_gbs = (double)blocks * threads * kIters * 4.0 / (ms * 1e-3) / 1e9;
-  rc = time_launch([&] { l1_probe<float4><<<blocks, threads>>>((const float4 *)src, out); }, 5, &ms);
+  rc = time_launch([&] { l1_probe<4><<<blocks, threads>>>(src, out); }, 5, &ms);
   if (rc) return rc;
   if (l1_16_gbs) *l1_16_gbs = (double)blocks * threads * kIters * 16.0 / (ms * 1e-3) / 1e9;
   rc = time_launch([&] { fma_probe<<<blocks, threads>>>(out, 0.999f, 0.001f); }, 5, &ms);
