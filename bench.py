@@ -46,7 +46,7 @@ WORKLOAD = "distance-driven pair, 2048x2048 image, 1800 angles [0,180), 2048 bin
 TAU_DD = 2  # gathered operand values per update (distance-driven)
 # DRAM bytes per launch of the two main kernels at 2048^2 x 1800, from one ncu capture
 # (dram__bytes_read.sum + dram__bytes_write.sum)
-DRAM_BYTES_PER_LAUNCH = {"forward": 520.66e6 + 19.07e6, "adjoint": 37.88e6 + 0.0192e6}
+DRAM_BYTES_PER_LAUNCH = {"forward": 139.65e6 + 15.33e6, "adjoint": 37.99e6 + 0.0064e6}
 
 
 def parse():
@@ -611,12 +611,12 @@ def c2_core(dev):
     return out
 
 
-def volume_core(dev, nslices=512, chunk=16, streams=3):
+def volume_core(dev, nslices=512, chunk=16, slots=3):
     """C4 volume: 512 slices of 2048 x 2048 at 1800 angles on [0, 180), 2048
     bins (a 7.55 GB float32 sinogram), held in page-locked host memory and
-    streamed through the GPU in chunks of ``chunk`` slices on ``streams`` CUDA
-    streams (streaming.VolumeStreamer): copy in, one multi-slice distance-
-    driven launch per chunk, copy out, overlapped across streams.  The forward
+    streamed through the GPU in chunks of ``chunk`` slices (streaming.
+    VolumeStreamer: a copy-in, a compute and a copy-out stream over ``slots``
+    buffer sets; one multi-slice distance-driven launch per chunk).  The forward
     projects the image volume, the adjoint backprojects the sinogram volume;
     each is timed end to end on the device (copies included) after a warm-up
     pass, beside the same launches on device-resident chunks (compute only):
@@ -634,14 +634,14 @@ def volume_core(dev, nslices=512, chunk=16, streams=3):
         imgs[z].copy_(base[z % 8])
     sinos = torch.empty((nslices, na, n), dtype=torch.float32).pin_memory()
     back = torch.empty((nslices, n, n), dtype=torch.float32).pin_memory()
-    vs = VolumeStreamer(tp, chunk=chunk, streams=streams, device=dev.index)
-    vs.project(imgs[:chunk * streams], sinos[:chunk * streams])      # warm-up: plans, tuning
-    vs.backproject(sinos[:chunk * streams], back[:chunk * streams])
+    vs = VolumeStreamer(tp, chunk=chunk, slots=slots, device=dev.index)
+    vs.project(imgs[:chunk * slots], sinos[:chunk * slots])      # warm-up: plans, tuning
+    vs.backproject(sinos[:chunk * slots], back[:chunk * slots])
     with ClockSampler(dev.index) as clk:
         ms_f = vs.project(imgs, sinos)
         ms_a = vs.backproject(sinos, back)
     # compute only: the same per-chunk launches on one resident chunk
-    plan = vs._plan(0, chunk)
+    plan = vs._plan(chunk)
     di, ds = vs._buf(0, "img"), vs._buf(0, "sino")
     di.copy_(imgs[:chunk])
     nchunks = (nslices + chunk - 1) // chunk
@@ -658,7 +658,7 @@ def volume_core(dev, nslices=512, chunk=16, streams=3):
     cf, ca = e0.elapsed_time(e1), e1.elapsed_time(e2)
     upd = float(nslices) * n * n * na
     out = {"config": f"{nslices} slices x {n}^2, {na} angles, {n} bins, dd pair, chunk {chunk} slices, "
-                     f"{streams} streams, page-locked host volume",
+                     f"copy-in / compute / copy-out streams over {slots} buffer sets, page-locked host volume",
            "sinogram_gb": nslices * na * n * 4 / 1e9, "image_gb": nslices * n * n * 4 / 1e9,
            "forward": {"ms": ms_f, "gups": upd / (ms_f * 1e-3) / 1e9, "compute_only_ms": cf, "overlap": cf / ms_f},
            "adjoint": {"ms": ms_a, "gups": upd / (ms_a * 1e-3) / 1e9, "compute_only_ms": ca, "overlap": ca / ms_a},

@@ -173,7 +173,8 @@ struct DdInst {
   const DdAngle *ang;    // [na] per-angle geometry, angle order
   const float4 *tab;     // adjoint lines: ROWS angles then COLS angles {r, k, z, v*w2 (int bits)}
   const int2 *tabS;      // adjoint sums: {mode, v*w2}
-  int n, nh, na, pads, w2, nR, nC, nS, ngrp, tx, ty, unused;
+  const int *fperm;      // forward angle order: the nRf angles on row lines first, then those on columns
+  int n, nh, na, pads, w2, nR, nC, nS, ngrp, tx, ty, nRf;
 };
 
 // Index of the instance whose range [key, next key) holds item (keys ascend).
@@ -645,9 +646,20 @@ __global__ void __launch_bounds__(32 * W, 28 / W) dd_fwd_kernel(const DdInst *__
     if (item - (BLOCK ? (threadIdx.x >> 5) : 0) >= nitems) break;  // block-uniform under BLOCK
     if (item < nitems) {
       const DdInst &I = inst[find_inst(inst, ninst, item, &DdInst::f0)];
-      const int local = (int)(item - I.f0);
-      dd_fwd_item(I, local % I.na, centre_out(local / I.na, I.ngrp), lane, work, sino, ep, item,
-                  xs[threadIdx.x >> 5]);
+      // items run all angles on row lines (every detector group) before those on
+      // column lines, so that the warps in flight read one of the two prefix
+      // tables at a time (each about half of L2 at 2048^2)
+      const int local = (int)(item - I.f0), nRg = I.nRf * I.ngrp;
+      int gi, v;
+      if (local < nRg) {
+        gi = local / I.nRf;
+        v = __ldg(I.fperm + local % I.nRf);
+      } else {
+        const int l2 = local - nRg, nCf = I.na - I.nRf;
+        gi = l2 / nCf;
+        v = __ldg(I.fperm + I.nRf + l2 % nCf);
+      }
+      dd_fwd_item(I, v, centre_out(gi, I.ngrp), lane, work, sino, ep, item, xs[threadIdx.x >> 5]);
     }
   }
 }
@@ -1024,8 +1036,8 @@ int dd_build(Plan &p, const DdGeo *geo, int count) {
   p.ext_free = dd_state_free;
   // host tables per geometry, packed into one device buffer
   struct GeoTabs {
-    size_t ang, tab, tabS;
-    int nR, nC, nS, pads, w2;
+    size_t ang, tab, tabS, fperm;
+    int nR, nC, nS, pads, w2, nRf;
   };
   std::vector<GeoTabs> gt(count);
   std::vector<char> blob;
@@ -1066,6 +1078,16 @@ int dd_build(Plan &p, const DdGeo *geo, int count) {
     t.nR = (int)rows.size();
     t.nC = (int)cols.size();
     t.nS = (int)sums.size();
+    // forward order: angles on row lines (ROWS, ROWSUM) first, each group in angle order
+    std::vector<int> fperm;
+    for (int pass = 0; pass < 2; ++pass)
+      for (int v = 0; v < na; ++v) {
+        const bool on_rows = tab[v].mode == DD_ROWS || tab[v].mode == DD_ROWSUM;
+        if (on_rows == (pass == 0)) fperm.push_back(v);
+      }
+    t.nRf = 0;
+    for (int v = 0; v < na; ++v) t.nRf += (tab[v].mode == DD_ROWS || tab[v].mode == DD_ROWSUM) ? 1 : 0;
+    t.fperm = put(fperm.data(), sizeof(int) * na);
     rows.insert(rows.end(), cols.begin(), cols.end());
     t.ang = put(tab.data(), sizeof(DdAngle) * na);
     t.tab = put(rows.data(), sizeof(float4) * rows.size());
@@ -1099,6 +1121,8 @@ int dd_build(Plan &p, const DdGeo *geo, int count) {
       I.ang = (const DdAngle *)(tb + t.ang);
       I.tab = (const float4 *)(tb + t.tab);
       I.tabS = (const int2 *)(tb + t.tabS);
+      I.fperm = (const int *)(tb + t.fperm);
+      I.nRf = t.nRf;
       I.img = (long long)io;
       I.sino = (long long)so;
       io += (size_t)G.n * G.n;

@@ -20,7 +20,7 @@ def test_project_and_backproject_match_per_slice(cuda, kind):
     rng = np.random.default_rng(1)
     imgs = torch.from_numpy(rng.standard_normal((nz, n, n)).astype(np.float32)).pin_memory()
     sinos = torch.empty((nz, na, n), dtype=torch.float32).pin_memory()
-    vs = VolumeStreamer(tp, chunk=3, streams=2)
+    vs = VolumeStreamer(tp, chunk=3, slots=2)
     ms = vs.project(imgs, sinos)
     assert ms > 0
     for z in range(nz):
@@ -42,7 +42,7 @@ def test_reconstruct_matches_per_slice_solver(cuda):
     truth = np.stack([random_ellipses(n, seed=s) for s in range(nz)])
     b = tp.A(truth)
     out = torch.empty((nz, n, n), dtype=torch.float32).pin_memory()
-    VolumeStreamer(tp, chunk=2, streams=3).reconstruct(torch.from_numpy(b).pin_memory(), out, "sirt", iters=7)
+    VolumeStreamer(tp, chunk=2, slots=3).reconstruct(torch.from_numpy(b).pin_memory(), out, "sirt", iters=7)
     for z in range(nz):
         x, _ = sirt(np.ones((n, n), np.float32), b[z], tp, n_iter=7)
         assert np.array_equal(out[z].numpy(), x), z
