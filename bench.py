@@ -65,9 +65,9 @@ def parse():
                     choices=["pair", "batch", "warmstart", "admm", "kinds", "peaks", "volume"],
                     help="pair: the dd pair at 2048^2 x 1800 (default); batch: batched uneven SIRT; "
                          "warmstart: learned warm start, time to the plain SIRT residual")
-    ap.add_argument("--train-pairs", type=int, default=1024, help="warmstart: training samples")
-    ap.add_argument("--train-steps", type=int, default=1500, help="warmstart: training steps")
-    ap.add_argument("--eval-slices", type=int, default=128, help="warmstart: held-out slices")
+    ap.add_argument("--train-pairs", type=int, default=2048, help="warmstart: training samples")
+    ap.add_argument("--train-steps", type=int, default=2000, help="warmstart: training steps")
+    ap.add_argument("--eval-slices", type=int, default=256, help="warmstart: held-out slices")
     ap.add_argument("--no-blocks", action="store_true",
                     help="pair workload: skip the C1-C5 blocks measured after the headline")
     ap.add_argument("--block-slices", type=int, default=512, help="C4 block: slices")

@@ -31,6 +31,37 @@ def random_ellipses(side: int, seed: int, count: int = 10, dtype=np.float32) -> 
     return img.astype(dtype)
 
 
+def random_ellipses_device(side: int, seeds, device, count: int = 10):
+    """``random_ellipses(side, seed)`` for every seed, drawn on the device: a
+    float32 tensor [len(seeds), side, side].  The ellipse parameters come from
+    the same numpy generator calls, and every pixel test is the same sequence of
+    float64 operations (each rounded, no fused multiply-add), so the images
+    equal the host ones."""
+    import torch
+    c = torch.from_numpy((np.arange(side) + 0.5) / side * 2.0 - 1.0).to(device)
+    X = c[None, :].expand(side, side)
+    Y = c.flip(0)[:, None].expand(side, side)
+    out = torch.empty((len(seeds), side, side), dtype=torch.float32, device=device)
+    for k, seed in enumerate(seeds):
+        rng = np.random.default_rng(seed)
+        img = torch.zeros((side, side), dtype=torch.float64, device=device)
+        for _ in range(count):
+            rad = np.sqrt(rng.uniform(0.0, 1.0))
+            ang = rng.uniform(0.0, 2 * np.pi)
+            x0, y0 = rad * np.cos(ang), rad * np.sin(ang)
+            a, b = rng.uniform(0.05, 0.5, size=2)
+            phi = rng.uniform(0.0, np.pi)
+            rho = rng.uniform(-0.5, 1.0)
+            cp, sp = np.cos(phi), np.sin(phi)
+            dx, dy = X - x0, Y - y0
+            xr = dx * cp + dy * sp
+            yr = -dx * sp + dy * cp
+            u, v = xr / a, yr / b
+            img += (u * u + v * v <= 1.0).to(torch.float64) * rho   # rho or 0, exactly
+        out[k] = img.clamp_(min=0.0).to(torch.float32)
+    return out
+
+
 def embed(img: np.ndarray, n_op: int) -> np.ndarray:
     """Centre ``img`` in an ``n_op`` x ``n_op`` zero canvas (edge-padding layout)."""
     side = img.shape[-1]

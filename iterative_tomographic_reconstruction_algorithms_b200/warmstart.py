@@ -36,7 +36,7 @@ import torch
 from . import nn
 from .autograd import Projector, sirt_unrolled, sirt_weights
 from .class_projectors_radon import projectors
-from .phantom import embed, random_ellipses
+from .phantom import random_ellipses_device
 from .solvers import Solver
 
 
@@ -54,12 +54,13 @@ class Problem:
 def make_batch(pb: Problem, seeds, device="cuda"):
     """(x_true, b, tp) for the given phantom seeds: float32 CUDA tensors [B, n_op, n_op], [B, na, n_op]."""
     tp = projectors(pb.n_op, np.linspace(0, 180, pb.na, endpoint=False), oper="dd")
-    imgs = []
-    for s in seeds:
-        ph = random_ellipses(pb.side, seed=int(s))
-        ph = ph / max(float(ph.max()), 1e-6) * pb.mu_max
-        imgs.append(embed(ph.astype(np.float32), pb.n_op))
-    x_true = torch.from_numpy(np.stack(imgs)).to(device)
+    # the phantoms of random_ellipses, drawn on the device (same values)
+    ph = random_ellipses_device(pb.side, [int(s) for s in seeds], device)
+    peak = ph.amax(dim=(1, 2), keepdim=True).clamp(min=1e-6)
+    ph = ph / peak * np.float32(pb.mu_max)
+    i1 = (pb.n_op - pb.side) // 2
+    x_true = torch.zeros((len(seeds), pb.n_op, pb.n_op), dtype=torch.float32, device=device)
+    x_true[:, i1:i1 + pb.side, i1:i1 + pb.side] = ph
     b_clean = tp.A(x_true)
     g = torch.Generator(device=device).manual_seed(int(seeds[0]) * 7919 + 1)
     counts = torch.poisson(pb.I0 * torch.exp(-b_clean), generator=g)

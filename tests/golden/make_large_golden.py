@@ -3,7 +3,8 @@
 
 Needs the compiled reference C (``make -C oracle ref``):
 
-    python tests/golden/make_large_golden.py
+    python tests/golden/make_large_golden.py           # Radon kinds and B-spline
+    python tests/golden/make_large_golden.py --grid    # gridding, large_grid_golden.npz
 
 A whole reference application at this size takes minutes (distance-driven:
 about 13 minutes), so the fixture samples it.  Every Radon and B-spline kernel
@@ -46,6 +47,7 @@ from iterative_tomographic_reconstruction_algorithms_b200.bspline_functions impo
 from iterative_tomographic_reconstruction_algorithms_b200.phantom import random_ellipses  # noqa: E402
 
 OUT = Path(__file__).resolve().parent / "large_golden.npz"
+OUT_GRID = Path(__file__).resolve().parent / "large_grid_golden.npz"
 N, NA = 2048, 1800
 ANGLE_INDEX = np.array([0, 1, 263, 449, 450, 451, 899, 900, 901, 1117, 1349, 1350, 1351, 1799])
 N_PIX = 32768
@@ -108,5 +110,50 @@ def main() -> None:
     print("wrote", OUT)
 
 
+# Gridding at the ADMM-TV configuration: 1536 bins, 1500 angles on [0, 180),
+# Kaiser-Bessel W = 6, oversampling 2 (a 4096^2 Fourier grid), linear
+# interpolation, no filter.  The forward's 2-D transform does not depend on the
+# angles and each angle's row is gathered from it alone, so the reference
+# called with the sampled angles gives their rows; its adjoint (no filter: the
+# filter factor is 1 whatever the angle count) is a sum over angles, so called
+# with the sampled rows it gives A^T of a sinogram zero outside them.
+N_GRID, NA_GRID = 1536, 1500
+GRID_INDEX = np.array([0, 1, 187, 374, 375, 376, 749, 750, 751, 1000, 1124, 1125, 1126, 1499])
+
+
+def grid_inputs():
+    """The seeded inputs of the gridding fixture (also used by the GPU test)."""
+    from iterative_tomographic_reconstruction_algorithms_b200.phantom import embed
+    phantom = embed(random_ellipses(1024, seed=2), N_GRID)
+    noise = np.random.default_rng(22).standard_normal((N_GRID, N_GRID), dtype=np.float32)
+    rows = np.random.default_rng(23).standard_normal((len(GRID_INDEX), N_GRID), dtype=np.float32)
+    pix = np.sort(np.random.default_rng(24).choice(N_GRID * N_GRID, size=N_PIX, replace=False))
+    return phantom, noise, rows, pix
+
+
+def grid_config():
+    from iterative_tomographic_reconstruction_algorithms_b200 import gridrec_lut as glut
+    Wp, lut, deapod = glut.configure_regridding(N_GRID, "kb", 2.0, "lin", 6.0, 1e-3)
+    param = np.array([0.0, 0, 0, 2.0, 1, len(lut) - 5, Wp, 0], np.float32)
+    return param, lut.astype(np.float32), deapod.astype(np.float32)
+
+
+def main_grid() -> None:
+    R = RefLib()
+    phantom, noise, rows, pix = grid_inputs()
+    param, lut, deapod = grid_config()
+    deg = np.linspace(0, 180, NA_GRID, endpoint=False).astype(np.float32)[GRID_INDEX]
+    data = {"angle_index": GRID_INDEX, "pix": pix.astype(np.int64),
+            "sums": np.array([x.sum(dtype=np.float64) for x in (phantom, noise, rows)]),
+            "fwd_phantom": R.gridrec(0, phantom, deg, param, lut, deapod),
+            "fwd_noise": R.gridrec(0, noise, deg, param, lut, deapod),
+            "adj": R.gridrec(1, rows, deg, param, lut, deapod).ravel()[pix]}
+    np.savez_compressed(OUT_GRID, **data)
+    print("wrote", OUT_GRID)
+
+
 if __name__ == "__main__":
-    main()
+    if "--grid" in sys.argv:
+        main_grid()
+    else:
+        main()

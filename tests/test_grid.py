@@ -166,3 +166,35 @@ def test_matched_adjoint_agrees_with_reference_on_band_limited_in_circle_data(cu
     disk = X ** 2 + Y ** 2 < 0.6 ** 2
     am, ac = tpm.At(y), tpc.At(y)
     assert rel_l2(am[disk], ac[disk]) <= 1e-2
+
+
+@pytest.mark.gpu
+def test_admm_size_sampled_angles_match_reference(cuda):
+    """The gridding pair at the ADMM-TV configuration (1536 bins, 1500 angles,
+    Kaiser-Bessel W = 6, oversampling 2: a 4096^2 Fourier grid, linear
+    interpolation): the full 1500-angle application on the GPU, its rows at 14
+    sampled angles and the adjoint of a sinogram zero outside them (at 32768
+    seeded pixels) against the reference (tests/golden/large_grid_golden.npz,
+    make_large_golden.py --grid)."""
+    import importlib.util
+    torch = cuda
+    from iterative_tomographic_reconstruction_algorithms_b200 import class_projectors_grid as cpg
+    spec = importlib.util.spec_from_file_location("make_large_golden", GOLDEN / "make_large_golden.py")
+    mk = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mk)
+    g = np.load(GOLDEN / "large_grid_golden.npz")
+    phantom, noise, rows, pix = mk.grid_inputs()
+    assert np.array_equal(np.array([x.sum(dtype=np.float64) for x in (phantom, noise, rows)]), g["sums"])
+    idx = g["angle_index"]
+    tp = cpg.projectors(mk.N_GRID, np.linspace(0, 180, mk.NA_GRID, endpoint=False), kernel="kb", oversampl=2.0,
+                        W=6.0, errs=1e-3, interp="lin", verbose=False)
+    for name, img in (("phantom", phantom), ("noise", noise)):
+        got = tp.A(torch.from_numpy(img).cuda()).cpu().numpy()[idx]
+        ref = g[f"fwd_{name}"]
+        assert rel_l2(got, ref) <= TOL, (name, rel_l2(got, ref))
+        for j in range(len(idx)):
+            assert rel_l2(got[j], ref[j]) <= TOL, (name, int(idx[j]), rel_l2(got[j], ref[j]))
+    y = torch.zeros((mk.NA_GRID, mk.N_GRID), dtype=torch.float32, device="cuda")
+    y[torch.from_numpy(idx).cuda()] = torch.from_numpy(rows).cuda()
+    adj = tp.At(y).cpu().numpy().ravel()[pix]
+    assert rel_l2(adj, g["adj"]) <= TOL, rel_l2(adj, g["adj"])
