@@ -12,12 +12,17 @@
   in-process pool whose ``apply_async(f, args)`` calls ``f(*args)`` at once (all
   slices can instead be passed as one [nz, n, n] array to the classes);
 * NumPy and SciPy names the scripts use that later releases removed:
-  ``np.int``, ``np.float``, ``np.bool``, ``np.complex``, ``np.object`` (read at
-  import, e.g. sir.py:68) and ``scipy.misc.factorial`` / ``comb``
-  (bspline_functions.py:76,155,183);
+  ``np.int``, ``np.float``, ``np.complex``, ``np.object`` (and ``np.bool`` on a
+  NumPy that lacks it; read at import, e.g. sir.py:68) and
+  ``scipy.misc.factorial`` / ``comb`` (bspline_functions.py:76,155,183);
 * plotting and image modules that are absent (matplotlib, pylab, skimage)
   become inert stand-ins: every attribute is a callable that returns another
-  stand-in, so ``plt.figure().add_subplot(111).imshow(...)`` does nothing.
+  stand-in, so ``plt.figure().add_subplot(111).imshow(...)`` does nothing;
+  except ``skimage.io.imread`` / ``imsave``, which read and write the scripts'
+  uncompressed float TIFFs;
+* the reference's compiled extensions outside the projector path that are not
+  built (its penalty module and split-Bregman NL-TV denoiser) import as
+  stand-ins whose functions raise when called.
 
 ``python -m iterative_tomographic_reconstruction_algorithms_b200.run
 path/to/sir.py [args]`` installs all of this, changes to the script's directory
@@ -122,6 +127,97 @@ class _Inert(types.ModuleType):
         return _Inert(f"{self.__name__}[]")
 
 
+class _MissingExtension(types.ModuleType):
+    """Stand-in for a compiled extension of the reference that is outside the
+    projector path (its regularisation penalties and its split-Bregman NL-TV
+    denoiser): importing it succeeds, so scripts that do not use it run; using
+    any of its functions raises."""
+
+    def __getattr__(self, name):
+        if name.startswith("__") and name.endswith("__"):
+            raise AttributeError(name)
+        mod = self.__name__
+
+        def missing(*args, **kwargs):
+            raise NotImplementedError(
+                f"{mod}.{name}: a compiled extension of the reference outside the projector path, "
+                f"which this package does not provide (build the reference's own module to use it)")
+        return missing
+
+
+class _ExtensionFinder:
+    """Meta-path finder, consulted after every other finder, that supplies
+    _MissingExtension modules for the reference's compiled extensions that are
+    not built: ``penalty`` (sir.py:46) and
+    ``pymodule_split_bregman_nltv.split_bregman_nltv`` (my_image_denoise.py:44)."""
+
+    NAMES = ("penalty", "pymodule_split_bregman_nltv.split_bregman_nltv")
+
+    def find_spec(self, fullname, path=None, target=None):
+        if fullname not in self.NAMES:
+            return None
+        import importlib.machinery
+        return importlib.machinery.ModuleSpec(fullname, self)
+
+    def create_module(self, spec):
+        return _MissingExtension(spec.name)
+
+    def exec_module(self, module):
+        pass
+
+
+def _tiff_imread(path):
+    """Reads a single-image, uncompressed TIFF of 32- or 64-bit floats (the
+    format the reference's scripts read and write with skimage.io), as a 2-D
+    numpy array."""
+    import struct
+
+    import numpy as np
+    raw = open(path, "rb").read()
+    end = "<" if raw[:2] == b"II" else ">"
+    off = struct.unpack_from(end + "I", raw, 4)[0]
+    count = struct.unpack_from(end + "H", raw, off)[0]
+    tags = {}
+    sizes = {3: ("H", 2), 4: ("I", 4)}
+    for i in range(count):
+        tag, typ, cnt, val = struct.unpack_from(end + "HHII", raw, off + 2 + 12 * i)
+        if typ in sizes:
+            fmt, size = sizes[typ]
+            at = off + 2 + 12 * i + 8 if cnt * size <= 4 else val
+            tags[tag] = struct.unpack_from(end + fmt * cnt, raw, at)
+    width, height = tags[256][0], tags[257][0]
+    bits, fmt = tags.get(258, (32,))[0], tags.get(339, (3,))[0]
+    if tags.get(259, (1,))[0] != 1:
+        raise ValueError(f"{path}: compressed TIFF is not supported")
+    kind = {1: "u", 2: "i", 3: "f"}[fmt]
+    dtype = np.dtype(f"{end}{kind}{bits // 8}")
+    data = b"".join(raw[o:o + c] for o, c in zip(tags[273], tags[279]))
+    return np.frombuffer(data, dtype=dtype, count=width * height).reshape(height, width).astype(dtype.newbyteorder("="))
+
+
+def _tiff_imsave(path, arr, **kwargs):
+    """Writes a 2-D float array as an uncompressed little-endian TIFF (float32
+    or float64)."""
+    import struct
+
+    import numpy as np
+    a = np.ascontiguousarray(arr)
+    if a.dtype not in (np.float32, np.float64):
+        a = a.astype(np.float32)
+    h, w = a.shape
+    body = a.astype(a.dtype.newbyteorder("<")).tobytes()
+    entries = [(256, 4, 1, w), (257, 4, 1, h), (258, 3, 1, a.itemsize * 8), (259, 3, 1, 1), (262, 3, 1, 1),
+               (273, 4, 1, 0), (277, 3, 1, 1), (278, 4, 1, h), (279, 4, 1, len(body)), (339, 3, 1, 3)]
+    ifd_off = 8
+    data_off = ifd_off + 2 + 12 * len(entries) + 4
+    out = bytearray(b"II*\x00" + struct.pack("<I", ifd_off) + struct.pack("<H", len(entries)))
+    for tag, typ, cnt, val in entries:
+        val = data_off if tag == 273 else val
+        out += struct.pack("<HHI", tag, typ, cnt) + (struct.pack("<HH", val, 0) if typ == 3 else struct.pack("<I", val))
+    out += struct.pack("<I", 0) + body
+    open(path, "wb").write(bytes(out))
+
+
 def _stub_if_absent(name: str) -> bool:
     try:
         importlib.import_module(name)
@@ -139,8 +235,10 @@ def install(classes: bool = True, pool: bool = True, stubs: bool = True) -> dict
     """Prepares the interpreter for the reference's scripts; returns what it did."""
     import numpy as np
     done = {"numpy_aliases": [], "stubs": [], "classes": [], "pool": False}
+    # only names NumPy no longer has: NumPy 2 defines np.bool again (its own
+    # bool scalar type, which numpy.ma relies on), so it is left alone
     for name, val in (("int", int), ("float", float), ("bool", bool), ("complex", complex), ("object", object)):
-        if not hasattr(np, name) or getattr(np, name) is not val:
+        if name not in vars(np):
             try:
                 setattr(np, name, val)
                 done["numpy_aliases"].append(name)
@@ -159,6 +257,14 @@ def install(classes: bool = True, pool: bool = True, stubs: bool = True) -> dict
                      "skimage", "skimage.io", "skimage.transform"):
             if _stub_if_absent(name):
                 done["stubs"].append(name)
+        if isinstance(sys.modules.get("skimage.io"), _Inert):
+            # the scripts read and write their float TIFFs with skimage.io
+            sys.modules["skimage.io"].imread = _tiff_imread
+            sys.modules["skimage.io"].imsave = _tiff_imsave
+            sys.modules["skimage"].io = sys.modules["skimage.io"]
+        if not any(isinstance(f, _ExtensionFinder) for f in sys.meta_path):
+            sys.meta_path.append(_ExtensionFinder())
+            done["stubs"] += list(_ExtensionFinder.NAMES)
     if classes:
         from . import class_projectors_bspline, class_projectors_grid, class_projectors_radon
         for mod in (class_projectors_radon, class_projectors_bspline, class_projectors_grid):

@@ -34,6 +34,14 @@ def main(argv=None) -> int:
     here = os.path.dirname(script)
     os.chdir(here)
     sys.path.insert(0, here)
+    # the reference's own Python modules next to the scripts (../common/...),
+    # which the scripts add to sys.path themselves, some only after importing
+    # from them (cg.py:28 before :42-44)
+    common = os.path.join(os.path.dirname(here), "common")
+    for sub in ("myimage", "operators/bspline_module", "operators/regularization_module", "operators/filters_module"):
+        d = os.path.join(common, sub)
+        if os.path.isdir(d) and d not in sys.path:
+            sys.path.append(d)
     runpy.run_path(script, run_name="__main__")
     return 0
 
