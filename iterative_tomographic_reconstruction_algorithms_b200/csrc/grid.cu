@@ -434,9 +434,14 @@ __device__ __forceinline__ void gather_point(const GatherArgs &A, int IU, int IV
       if (si >= na) si -= na;
       const float2 e = A.sorted[si];
       if (windowed) {
+        // Stop once past the window.  The test is looser than the window by
+        // far more than the float rounding of lo = phi - dmax and of e.x - phi:
+        // the search starts at the first angle >= lo, which the exact test
+        // could judge just outside and so end the scan before the window.
+        // Which samples count is decided below, per sample, whatever this.
         float dphi = fabsf(e.x - phi);
         dphi = fminf(dphi, 6.2831853f - dphi);
-        if (dphi > dmax) break;  // left the window
+        if (dphi > dmax + 1e-5f) break;  // left the window
       }
       const int n = __float_as_int(e.y);
       const float4 ang = A.sc4[n];  // SIN, COS, 1/COS, 1/SIN
