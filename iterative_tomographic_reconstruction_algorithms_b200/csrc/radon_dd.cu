@@ -168,6 +168,7 @@ struct DdInst {
   long long img, sino;   // offsets (floats) of the image / sinogram in the packed arrays
   long long sl;          // offset (double2) of the row prefix lines; column lines follow
   long long as;          // offset (double2) of the sinogram prefix rows [na][w2]
+  long long xs;          // offset (double2) of the forward's width corrections, float [na][n]
   long long f0, a0;      // first forward / adjoint work item
   long long r0, c0, s0;  // first row-prefix / column-prefix / sinogram-prefix block
   const DdAngle *ang;    // [na] per-angle geometry, angle order
@@ -419,14 +420,16 @@ __device__ __forceinline__ int dd_fwd_kk(float lo_nh, float q, float nlim) {
 // near-axis angles reach (q = y k with |k| up to 1/|cos|).  dd_fwd_lines
 // integrates unit widths, so on each line the detector m whose boundary
 // indices bracket such a pixel j (kk_m <= j < kk_m+1, the loop's own kk) is
-// short by delta * L_j.  This adds those amounts for the item's detectors to
-// X[m - B0] (the warp's shared-memory row, zeroed by the caller).  A crossing is taken at P = +-2^e, e >= 0, each
+// short by delta * L_j.  This adds those amounts for the detectors [B0, mEnd)
+// to X[m - B0] (a row of the angle's corrections in global memory, zeroed by
+// the caller); only lane 0 writes, crossing after crossing, so the sums are
+// deterministic.  A crossing is taken at P = +-2^e, e >= 0, each
 // pixel at the smallest one it straddles; below |P| = 1 deltas are < 2^-23.
 // Lanes take the lines of one crossing in turn; the four sums per crossing
 // (the detector holding the crossing and its neighbours) are reduced over the
 // warp in a fixed order, so the result is deterministic.
 __device__ __forceinline__ void dd_fwd_crossings(const double2 *__restrict__ SL, int ws, float k, float r, int n,
-                                                 int nh, int B0, int mEnd, int lane, double *__restrict__ X) {
+                                                 int nh, int B0, int mEnd, int lane, float *__restrict__ X) {
   const float DA = det_bound(B0, nh, r), DB = det_bound(mEnd, nh, r);
   const float nlim = (float)n + 0.25f, fnh = (float)nh;
 #pragma unroll 1
@@ -487,7 +490,7 @@ __device__ __forceinline__ void dd_fwd_crossings(const double2 *__restrict__ SL,
         double v = a[t];
         for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
         const int rel = mc - 1 + t - B0;
-        if (lane == 0 && mc - 1 + t < mEnd && rel >= 0) X[rel] += v;
+        if (lane == 0 && mc - 1 + t < mEnd && rel >= 0) X[rel] += (float)v;
       }
       __syncwarp();
     }
@@ -501,7 +504,7 @@ __device__ __forceinline__ void dd_fwd_crossings(const double2 *__restrict__ SL,
 // meeting it, the overlap pieces of the detector with the line's pixels, from
 // the same float boundaries as the reference, the dropped last piece skipped
 // (radon_dd.c:125-189), summed in double.
-__device__ __noinline__ void dd_fwd_exact(const double2 *__restrict__ SL, int ws, float k, float r, int n, int nh,
+__device__ __forceinline__ void dd_fwd_exact(const double2 *__restrict__ SL, int ws, float k, float r, int n, int nh,
                                           int B0, int mEnd, int lane, double (&T)[4]) {
   const float Dn = det_bound(n, nh, r);
 #pragma unroll 1
@@ -535,9 +538,33 @@ __device__ __noinline__ void dd_fwd_exact(const double2 *__restrict__ SL, int ws
   }
 }
 
+// The binade corrections of every angle (dd_fwd_crossings over all detectors),
+// one warp per angle of every instance, into the float rows X[v][m] that the
+// forward adds where it stores.  A separate launch, so that the forward's
+// register budget is that of its main loop.
+__device__ __forceinline__ bool dd_wide(float k, int nh) {
+  return fabsf(k) * (float)(nh + 1) + (float)(nh + 2) >= 4194304.0f;
+}
+
+__global__ void __launch_bounds__(128) dd_fwd_corr_kernel(const DdInst *__restrict__ inst, int ninst,
+                                                          long long nangles, double2 *__restrict__ work) {
+  const long long gw = (long long)blockIdx.x * 4 + (threadIdx.x >> 5);
+  if (gw >= nangles) return;  // warp-uniform
+  const int lane = threadIdx.x & 31;
+  const DdInst &I = inst[find_inst(inst, ninst, gw, &DdInst::s0)];
+  const int v = (int)(gw - I.s0), n = I.n, nh = I.nh, ws = n + 2;
+  float *X = reinterpret_cast<float *>(work + I.xs) + (size_t)v * n;
+  for (int m = lane; m < n; m += 32) X[m] = 0.0f;
+  __syncwarp();
+  const DdAngle g = I.ang[v];
+  if ((g.mode != DD_ROWS && g.mode != DD_COLS) || dd_wide(g.k, nh)) return;
+  const double2 *SLr = work + I.sl + 1, *SL = g.mode == DD_ROWS ? SLr : SLr + (size_t)n * ws;
+  dd_fwd_crossings(SL, ws, g.k, g.r, n, nh, 0, n, lane, X);
+}
+
 __device__ __forceinline__ void dd_fwd_item(const DdInst &I, int v, int grp, int lane,
                                             const double2 *__restrict__ work, float *__restrict__ sino,
-                                            const FwdEpi &ep, long long slot, double *__restrict__ xs) {
+                                            const FwdEpi &ep, long long slot) {
   const DdAngle g = I.ang[v];
   const int n = I.n, nh = I.nh, ws = n + 2;
   const int B0 = grp * kGrpDet;
@@ -573,17 +600,13 @@ __device__ __forceinline__ void dd_fwd_item(const DdInst &I, int v, int grp, int
       j0 = i1 + 1;
       j1 = i1;
     }
-    if (fabsf(k) * (float)(nh + 1) + (float)(nh + 2) >= 4194304.0f) {
+    if (dd_wide(k, nh)) {
       // |P| reaches 2^22: pieces walked exactly (rare near-axis angles)
       double T[4] = {0.0, 0.0, 0.0, 0.0};
       dd_fwd_exact(SL, ws, k, r, n, nh, B0, mEnd, lane, T);
 #pragma unroll
       for (int j = 0; j < 4; ++j) acc[j] = (float)T[j];
     } else {
-#pragma unroll
-      for (int j = 0; j < 4; ++j) xs[32 * j + lane] = 0.0;
-      __syncwarp();
-      dd_fwd_crossings(SL, ws, k, r, n, nh, B0, mEnd, lane, xs);
       double T[4] = {0.0, 0.0, 0.0, 0.0}, C[4] = {0.0, 0.0, 0.0, 0.0};
       dd_fwd_lines<false>(i0, j0, SL, ws, k, r, n, nh, B0, lane, Dlo, lo_nh, T, C);
       dd_fwd_lines<true>(j0, j1 + 1, SL, ws, k, r, n, nh, B0, lane, Dlo, lo_nh, T, C);
@@ -594,7 +617,11 @@ __device__ __forceinline__ void dd_fwd_item(const DdInst &I, int v, int grp, int
         const double a = __shfl_down_sync(0xffffffffu, T[j], 1);
         const double b = __shfl_sync(0xffffffffu, j < 3 ? T[j < 3 ? j + 1 : 3] : 0.0, 0);
         const double up = lane < 31 ? a : b;
-        acc[j] = (float)(((up - T[j]) - C[j]) + xs[32 * j + lane]);
+        const int m = B0 + 32 * j + lane;
+        const float x = (32 * j + lane < kGrpDet && m < n)
+                            ? __ldg(reinterpret_cast<const float *>(work + I.xs) + (size_t)v * n + m)
+                            : 0.0f;
+        acc[j] = (float)(((up - T[j]) - C[j]) + (double)x);
       }
     }
   }
@@ -634,12 +661,11 @@ __device__ __forceinline__ int centre_out(int gi, int ngrp) {
 }
 
 template <int W, bool BLOCK>
-__global__ void __launch_bounds__(32 * W, 28 / W) dd_fwd_kernel(const DdInst *__restrict__ inst, int ninst,
+__global__ void __launch_bounds__(32 * W) dd_fwd_kernel(const DdInst *__restrict__ inst, int ninst,
                                                          long long nitems, unsigned long long *__restrict__ ctr,
                                                          const double2 *__restrict__ work,
                                                          float *__restrict__ sino, FwdEpi ep) {
   __shared__ long long base_s;
-  __shared__ double xs[W][128];  // per warp: binade corrections of its item's detectors
   const int lane = threadIdx.x & 31;
   for (;;) {
     const long long item = fetch_item<BLOCK>(ctr, W, &base_s);
@@ -659,7 +685,7 @@ __global__ void __launch_bounds__(32 * W, 28 / W) dd_fwd_kernel(const DdInst *__
         gi = l2 / nCf;
         v = __ldg(I.fperm + I.nRf + l2 % nCf);
       }
-      dd_fwd_item(I, v, centre_out(gi, I.ngrp), lane, work, sino, ep, item, xs[threadIdx.x >> 5]);
+      dd_fwd_item(I, v, centre_out(gi, I.ngrp), lane, work, sino, ep, item);
     }
   }
 }
@@ -1143,12 +1169,16 @@ int dd_build(Plan &p, const DdGeo *geo, int count) {
   for (int idx : order) work += 2 * (size_t)inst[idx].n * (inst[idx].n + 2);
   size_t sl_at = 0, as_at = work;
   for (int idx : order) work += (size_t)inst[idx].na * inst[idx].w2;
+  size_t xs_at = work;  // float rows, 4 to a double2
+  for (int idx : order) work += ((size_t)inst[idx].na * inst[idx].n + 3) / 4;
   for (int idx : order) {
     DdInst I = inst[idx];
     I.sl = (long long)sl_at;
     sl_at += 2 * (size_t)I.n * (I.n + 2);
     I.as = (long long)as_at;
     as_at += (size_t)I.na * I.w2;
+    I.xs = (long long)xs_at;
+    xs_at += ((size_t)I.na * I.n + 3) / 4;
     I.f0 = S->fwd_items;
     S->fwd_items += (long long)I.na * I.ngrp;
     I.a0 = S->adj_items;
@@ -1231,6 +1261,7 @@ int dd_forward(Plan &p, const float *d_img, float *d_sino, cudaStream_t s, const
   const int ni = (int)S.inst.size();
   dd_row_prefix_kernel<<<(unsigned)S.row_blocks, kScanThreads, 0, s>>>(S.d_inst, ni, d_img, work);
   dd_col_prefix_kernel<<<(unsigned)S.col_blocks, 32 * kColWarps, 0, s>>>(S.d_inst, ni, d_img, work);
+  dd_fwd_corr_kernel<<<(unsigned)((S.sino_blocks + 3) / 4), 128, 0, s>>>(S.d_inst, ni, S.sino_blocks, work);
   TOMO_CUDA(cudaGetLastError());
   return dd_launch_fwd(S, S.wf, S.grid_f, work, d_sino, s, ep);
 }
