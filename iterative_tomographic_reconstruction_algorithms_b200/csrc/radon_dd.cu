@@ -27,7 +27,7 @@
 //            reference's are P_j+1 - P_j in float, which is 1 exactly except
 //            for pixels straddling a binade of P (|P| = 2^e), whose width
 //            differs by a rounding of q: those are added per line
-//            (dd_fwd_crossings).  Angles whose coordinates reach 2^22 walk
+//            (dd_fwd_corr_kernel).  Angles whose coordinates reach 2^22 walk
 //            the pieces instead (dd_fwd_exact).
 //   adjoint  a pixel is at most one detector wide (r >= 1), so it overlaps the
 //            detector holding its left boundary and possibly the next: two
@@ -45,6 +45,7 @@
 // candidates (dd_autotune).  The projection arithmetic of the solvers
 // (epilogue.cuh) is applied where the result is stored.
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -428,73 +429,71 @@ __device__ __forceinline__ int dd_fwd_kk(float lo_nh, float q, float nlim) {
 // Lanes take the lines of one crossing in turn; the four sums per crossing
 // (the detector holding the crossing and its neighbours) are reduced over the
 // warp in a fixed order, so the result is deterministic.
-__device__ __forceinline__ void dd_fwd_crossings(const double2 *__restrict__ SL, int ws, float k, float r, int n,
-                                                 int nh, int B0, int mEnd, int lane, float *__restrict__ X) {
-  const float DA = det_bound(B0, nh, r), DB = det_bound(mEnd, nh, r);
+// One crossing, c = 2 e + (B < 0), B = +-2^e: false if no detector of the
+// angle can get a correction from it; otherwise mc (the detector holding B)
+// and, in every lane, the warp's sums for detectors mc-1 .. mc+2 (a fixed
+// butterfly, so deterministic).
+constexpr int kNumCrossings = 46;  // e = 0 .. 22, both signs
+
+__device__ __forceinline__ bool dd_fwd_crossing(const double2 *__restrict__ SL, int ws, float k, float r, int n,
+                                                int nh, int c, int lane, int &mc, double (&a)[4]) {
+  const int e = c >> 1, sg = c & 1;
+  const float DA = det_bound(0, nh, r), DB = det_bound(n, nh, r);
   const float nlim = (float)n + 0.25f, fnh = (float)nh;
-#pragma unroll 1
-  for (int e = 0; e <= 22; ++e) {
-#pragma unroll 1
-    for (int sg = 0; sg < 2; ++sg) {
-      const float B = sg ? -ldexpf(1.0f, e) : ldexpf(1.0f, e);
-      if (!(B >= DA - 3.0f && B <= DB + 3.0f)) continue;  // warp-uniform
-      // detector holding B: D_mc <= B < D_mc+1
-      int mc = (int)floor((double)B / (double)r) + nh;
-      for (int it = 0; it < 4 && det_bound(mc, nh, r) > B; ++it) --mc;
-      for (int it = 0; it < 4 && det_bound(mc + 1, nh, r) <= B; ++it) ++mc;
-      // lines on which the crossing lies within [P_0, P_n]: q in [-nh - B - 2, n - nh - B + 2]
-      int ia, ib;
-      dd_line_range(-(double)nh - B - 2.0, (double)(n - nh) - B + 2.0, (double)k, n, nh, ia, ib);
-      // and on which delta can be nonzero: a float q with |q| >= 2^e is a
-      // multiple of both binades' spacings (2^(e-24), 2^(e-23)), so then both
-      // roundings are exact and the width is 1: only |y k| < 2^e matters
-      const double ymax = ldexp(1.0, e) * (1.0 + 1e-6) / fabs((double)k) + 1.0;
-      if (ymax < (double)n) {
-        ia = max(ia, (int)floor((double)nh - 0.5 - ymax));
-        ib = min(ib, (int)ceil((double)nh - 0.5 + ymax));
-      }
-      double a[4] = {0.0, 0.0, 0.0, 0.0};
-#pragma unroll 1
-      for (int i = ia + lane; i <= ib; i += 32) {
-        const float q = __fmul_rn(__fadd_rn((float)(i - nh), 0.5f), k);
-        int j = (int)floor((double)B + (double)q) + nh - 1;
-        // j with P_j < B <= P_j+1 (B > 0) or P_j <= B < P_j+1 (B < 0)
-        if (!sg) {
-          for (int it = 0; it < 4 && pix_bound(j, nh, q) >= B; ++it) --j;
-          for (int it = 0; it < 4 && pix_bound(j + 1, nh, q) < B; ++it) ++j;
-        } else {
-          for (int it = 0; it < 4 && pix_bound(j, nh, q) > B; ++it) --j;
-          for (int it = 0; it < 4 && pix_bound(j + 1, nh, q) <= B; ++it) ++j;
-        }
-        if (j < 0 || j >= n) continue;
-        const float Pj = pix_bound(j, nh, q), Pj1 = pix_bound(j + 1, nh, q);
-        const bool at = sg ? (Pj <= B && B < Pj1 && (e == 0 || Pj1 <= 0.5f * B))
-                           : (Pj < B && B <= Pj1 && (e == 0 || Pj >= 0.5f * B));
-        if (!at) continue;
-        const float delta = __fsub_rn(__fsub_rn(Pj1, Pj), 1.0f);
-        if (delta == 0.0f) continue;
-        // the detector m with kk_m <= j < kk_m+1, among mc-1 .. mc+2
-        int m = mc;
-        for (int it = 0; it < 4; ++it) {
-          if (dd_fwd_kk(__fadd_rn(det_bound(m, nh, r), fnh), q, nlim) > j) --m;
-          else if (dd_fwd_kk(__fadd_rn(det_bound(m + 1, nh, r), fnh), q, nlim) <= j) ++m;
-          else break;
-        }
-        const double amt = (double)delta * __ldg(&SL[(size_t)i * ws + j].y);
-#pragma unroll
-        for (int t = 0; t < 4; ++t)
-          if (m == mc - 1 + t) a[t] += amt;
-      }
-#pragma unroll
-      for (int t = 0; t < 4; ++t) {
-        double v = a[t];
-        for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-        const int rel = mc - 1 + t - B0;
-        if (lane == 0 && mc - 1 + t < mEnd && rel >= 0) X[rel] += (float)v;
-      }
-      __syncwarp();
-    }
+  const float B = sg ? -ldexpf(1.0f, e) : ldexpf(1.0f, e);
+  if (!(B >= DA - 3.0f && B <= DB + 3.0f)) return false;
+  // detector holding B: D_mc <= B < D_mc+1
+  mc = (int)floor((double)B / (double)r) + nh;
+  for (int it = 0; it < 4 && det_bound(mc, nh, r) > B; ++it) --mc;
+  for (int it = 0; it < 4 && det_bound(mc + 1, nh, r) <= B; ++it) ++mc;
+  // lines on which the crossing lies within [P_0, P_n]: q in [-nh - B - 2, n - nh - B + 2]
+  int ia, ib;
+  dd_line_range(-(double)nh - B - 2.0, (double)(n - nh) - B + 2.0, (double)k, n, nh, ia, ib);
+  // and on which delta can be nonzero: a float q with |q| >= 2^e is a
+  // multiple of both binades' spacings (2^(e-24), 2^(e-23)), so then both
+  // roundings are exact and the width is 1: only |y k| < 2^e matters
+  const double ymax = ldexp(1.0, e) * (1.0 + 1e-6) / fabs((double)k) + 1.0;
+  if (ymax < (double)n) {
+    ia = max(ia, (int)floor((double)nh - 0.5 - ymax));
+    ib = min(ib, (int)ceil((double)nh - 0.5 + ymax));
   }
+#pragma unroll
+  for (int t = 0; t < 4; ++t) a[t] = 0.0;
+#pragma unroll 1
+  for (int i = ia + lane; i <= ib; i += 32) {
+    const float q = __fmul_rn(__fadd_rn((float)(i - nh), 0.5f), k);
+    int j = (int)floor((double)B + (double)q) + nh - 1;
+    // j with P_j < B <= P_j+1 (B > 0) or P_j <= B < P_j+1 (B < 0)
+    if (!sg) {
+      for (int it = 0; it < 4 && pix_bound(j, nh, q) >= B; ++it) --j;
+      for (int it = 0; it < 4 && pix_bound(j + 1, nh, q) < B; ++it) ++j;
+    } else {
+      for (int it = 0; it < 4 && pix_bound(j, nh, q) > B; ++it) --j;
+      for (int it = 0; it < 4 && pix_bound(j + 1, nh, q) <= B; ++it) ++j;
+    }
+    if (j < 0 || j >= n) continue;
+    const float Pj = pix_bound(j, nh, q), Pj1 = pix_bound(j + 1, nh, q);
+    const bool at = sg ? (Pj <= B && B < Pj1 && (e == 0 || Pj1 <= 0.5f * B))
+                       : (Pj < B && B <= Pj1 && (e == 0 || Pj >= 0.5f * B));
+    if (!at) continue;
+    const float delta = __fsub_rn(__fsub_rn(Pj1, Pj), 1.0f);
+    if (delta == 0.0f) continue;
+    // the detector m with kk_m <= j < kk_m+1, among mc-1 .. mc+2
+    int m = mc;
+    for (int it = 0; it < 4; ++it) {
+      if (dd_fwd_kk(__fadd_rn(det_bound(m, nh, r), fnh), q, nlim) > j) --m;
+      else if (dd_fwd_kk(__fadd_rn(det_bound(m + 1, nh, r), fnh), q, nlim) <= j) ++m;
+      else break;
+    }
+    const double amt = (double)delta * __ldg(&SL[(size_t)i * ws + j].y);
+#pragma unroll
+    for (int t = 0; t < 4; ++t)
+      if (m == mc - 1 + t) a[t] += amt;
+  }
+#pragma unroll
+  for (int t = 0; t < 4; ++t)
+    for (int o = 16; o; o >>= 1) a[t] += __shfl_xor_sync(0xffffffffu, a[t], o);
+  return true;
 }
 
 // An item of an angle whose pixel coordinates reach |P| >= 2^22 (|cos| or
@@ -538,28 +537,60 @@ __device__ __forceinline__ void dd_fwd_exact(const double2 *__restrict__ SL, int
   }
 }
 
-// The binade corrections of every angle (dd_fwd_crossings over all detectors),
-// one warp per angle of every instance, into the float rows X[v][m] that the
-// forward adds where it stores.  A separate launch, so that the forward's
+// The binade corrections of every angle into the float rows X[v][m] that the
+// forward adds where it stores: one block per angle of every instance, its
+// warps taking the crossings in turn (dd_fwd_crossing); the crossings' sums
+// are then added into the row in crossing order through shared memory, so the
+// result is deterministic.  A launch of its own, so that the forward's
 // register budget is that of its main loop.
 __device__ __forceinline__ bool dd_wide(float k, int nh) {
   return fabsf(k) * (float)(nh + 1) + (float)(nh + 2) >= 4194304.0f;
 }
 
-__global__ void __launch_bounds__(128) dd_fwd_corr_kernel(const DdInst *__restrict__ inst, int ninst,
-                                                          long long nangles, double2 *__restrict__ work) {
-  const long long gw = (long long)blockIdx.x * 4 + (threadIdx.x >> 5);
-  if (gw >= nangles) return;  // warp-uniform
-  const int lane = threadIdx.x & 31;
-  const DdInst &I = inst[find_inst(inst, ninst, gw, &DdInst::s0)];
-  const int v = (int)(gw - I.s0), n = I.n, nh = I.nh, ws = n + 2;
+constexpr int kCorrWarps = 8, kCorrRow = 4096;  // rows longer than kCorrRow are added in global memory
+
+__global__ void __launch_bounds__(32 * kCorrWarps) dd_fwd_corr_kernel(const DdInst *__restrict__ inst, int ninst,
+                                                                      double2 *__restrict__ work) {
+  __shared__ double sums[kNumCrossings][4];
+  __shared__ int smc[kNumCrossings];
+  __shared__ float row[kCorrRow];
+  const long long b = blockIdx.x;
+  const DdInst &I = inst[find_inst(inst, ninst, b, &DdInst::s0)];
+  const int v = (int)(b - I.s0), n = I.n, nh = I.nh, ws = n + 2;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   float *X = reinterpret_cast<float *>(work + I.xs) + (size_t)v * n;
-  for (int m = lane; m < n; m += 32) X[m] = 0.0f;
-  __syncwarp();
   const DdAngle g = I.ang[v];
-  if ((g.mode != DD_ROWS && g.mode != DD_COLS) || dd_wide(g.k, nh)) return;
+  const bool lines = (g.mode == DD_ROWS || g.mode == DD_COLS) && !dd_wide(g.k, nh);
   const double2 *SLr = work + I.sl + 1, *SL = g.mode == DD_ROWS ? SLr : SLr + (size_t)n * ws;
-  dd_fwd_crossings(SL, ws, g.k, g.r, n, nh, 0, n, lane, X);
+  for (int c = warp; c < kNumCrossings; c += kCorrWarps) {
+    int mc = 0;
+    double a[4] = {0.0, 0.0, 0.0, 0.0};
+    const bool used = lines && dd_fwd_crossing(SL, ws, g.k, g.r, n, nh, c, lane, mc, a);
+    if (lane == 0) {
+      smc[c] = used ? mc : INT_MIN;
+#pragma unroll
+      for (int t = 0; t < 4; ++t) sums[c][t] = a[t];
+    }
+  }
+  const bool in_smem = n <= kCorrRow;
+  for (int m = threadIdx.x; m < n; m += blockDim.x) {
+    if (in_smem) row[m] = 0.0f;
+    else X[m] = 0.0f;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float *R = in_smem ? row : X;
+    for (int c = 0; c < kNumCrossings; ++c) {
+      if (smc[c] == INT_MIN) continue;
+      for (int t = 0; t < 4; ++t) {
+        const int m = smc[c] - 1 + t;
+        if (m >= 0 && m < n) R[m] += (float)sums[c][t];
+      }
+    }
+  }
+  __syncthreads();
+  if (in_smem)
+    for (int m = threadIdx.x; m < n; m += blockDim.x) X[m] = row[m];
 }
 
 __device__ __forceinline__ void dd_fwd_item(const DdInst &I, int v, int grp, int lane,
@@ -1261,7 +1292,7 @@ int dd_forward(Plan &p, const float *d_img, float *d_sino, cudaStream_t s, const
   const int ni = (int)S.inst.size();
   dd_row_prefix_kernel<<<(unsigned)S.row_blocks, kScanThreads, 0, s>>>(S.d_inst, ni, d_img, work);
   dd_col_prefix_kernel<<<(unsigned)S.col_blocks, 32 * kColWarps, 0, s>>>(S.d_inst, ni, d_img, work);
-  dd_fwd_corr_kernel<<<(unsigned)((S.sino_blocks + 3) / 4), 128, 0, s>>>(S.d_inst, ni, S.sino_blocks, work);
+  dd_fwd_corr_kernel<<<(unsigned)S.sino_blocks, 32 * kCorrWarps, 0, s>>>(S.d_inst, ni, work);
   TOMO_CUDA(cudaGetLastError());
   return dd_launch_fwd(S, S.wf, S.grid_f, work, d_sino, s, ep);
 }
