@@ -12,7 +12,7 @@
 // to the pixel it steps INTO (x index -> image row) if that pixel has row and
 // column in [1, n-1]; it stops after the first step with alpha > 1.
 //
-// Both directions run the same walks (rd_walk), one thread per (bin, angle,
+// Both directions run the same walks (rd_walk_loop), one thread per (bin, angle,
 // slice) replaying its bin's five sub-rays:
 //   forward  gathers 0.2 l x[pixel] into the bin, in walk order;
 //   adjoint  scatters 0.2 l y[bin] into a 64-bit fixed-point image with
@@ -28,7 +28,7 @@
 // the image (forward) and scatter into a transposed fixed-point image
 // (adjoint), so neighbouring lanes touch neighbouring words.
 // The walk's arithmetic is float only: the crossing parameters reproduce the
-// reference's double quotients exactly (rd_alpha_ff), with a double division
+// reference's double quotients exactly (rd_alpha_mf), with a double division
 // only for quotients within 2^-38 of a float rounding boundary.
 #include <algorithm>
 #include <cmath>
@@ -62,7 +62,7 @@ __device__ __forceinline__ int rd_round_i(float x) {
 // Entry point, extents, start pixel and step directions of a sub-ray at
 // offset t (radon_rd.c:133-179 and :21-36); the walk computes its length.
 struct RdGeom {
-  float p1x, p1y, ex, ey;
+  float p1x, p1y, p2x, p2y, ex, ey;
   int ii0, jj0, dx, dy;
 };
 
@@ -83,6 +83,8 @@ __device__ __forceinline__ RdGeom rd_geom(float t, const RdAngle &g, int nh) {
   RdGeom r;
   r.p1x = p1x;
   r.p1y = p1y;
+  r.p2x = p2x;
+  r.p2y = p2y;
   r.ex = __fsub_rn(p2x, p1x);
   r.ey = __fsub_rn(p2y, p1y);
   r.ii0 = rd_round_i(p1x);
@@ -92,30 +94,32 @@ __device__ __forceinline__ RdGeom rd_geom(float t, const RdAngle &g, int nh) {
   return r;
 }
 
-// The double division of rd_alpha_ff, out of line: rarely taken, and its
+// The double division of rd_alpha_mf, out of line: rarely taken, and its
 // double registers stay out of the walk loops.
 __device__ __noinline__ float rd_alpha_div(float h, float l, float e) {
   return __double2float_rn(__ddiv_rn(__dadd_rn((double)h, (double)l), (double)e));
 }
 
-// alpha of the crossing at the half-integer coordinate a, for a sub-ray that
-// enters at p with extent e, r = RN(1/e): the float of the correctly rounded
-// double quotient ((double)a - p) / e that the reference computes
-// (radon_rd.c:41-42), in float arithmetic.
+// alpha of a crossing, for a sub-ray that enters at p with extent e,
+// r = RN(1/e): the float of the correctly rounded double quotient
+// ((double)a - p) / e that the reference computes (radon_rd.c:41-42), a the
+// crossing's half-integer coordinate, in float arithmetic.  The numerator is
+// given as m - f with p = P + f, P = rint(p), |f| <= 1/2 (exact), and
+// m = a - P, a half-integer (exact), which the walk steps by +-1.
 //
-// a - p = h + l exactly (Knuth's TwoSum).  q1 = RN(h r); the remainder
-// h + l - q1 e (one FMA, then + l) times r gives q2, and q1 + q2 is within
-// 2^-44 |x| of the exact quotient x (r and q1 are within 2^-23 of exact, the
-// remainder is 2^-23 |h| small).  With d = 2^-38 |q1|, RN(q1 + RN(q2 - d))
-// and RN(q1 + RN(q2 + d)) round points below and above every value within
-// 2^-44 |x| of q1 + q2 (the inner roundings move them by 2^-47 at most).
-// Rounding to nearest is monotone, so when both give the same float s, x and
-// the double nearest x (2^-53 |x| from it) round to s too.  Otherwise (x within
-// about 2^-38 of a float rounding boundary, or e zero) divide in double.
-__device__ __forceinline__ float rd_alpha_ff(float a, float p, float e, float r) {
-  const float h = __fsub_rn(a, p);
-  const float bb = __fsub_rn(h, a);
-  const float l = __fadd_rn(__fsub_rn(a, __fsub_rn(h, bb)), __fsub_rn(-p, bb));
+// a - p = m - f = h + l exactly (Fast2Sum, valid since |m| >= 1/2 >= |f|).
+// q1 = RN(h r); the remainder h + l - q1 e (one FMA, then + l) times r gives
+// q2, and q1 + q2 is within 2^-44 |x| of the exact quotient x (r and q1 are
+// within 2^-23 of exact, the remainder is 2^-23 |h| small).  With
+// d = 2^-38 |q1|, RN(q1 + RN(q2 - d)) and RN(q1 + RN(q2 + d)) round points
+// below and above every value within 2^-44 |x| of q1 + q2 (the inner roundings
+// move them by 2^-47 at most).  Rounding to nearest is monotone, so when both
+// give the same float s, x and the double nearest x (2^-53 |x| from it) round
+// to s too.  Otherwise (x within about 2^-38 of a float rounding boundary, or
+// e zero) divide in double.
+__device__ __forceinline__ float rd_alpha_mf(float m, float f, float e, float r) {
+  const float h = __fsub_rn(m, f);
+  const float l = __fsub_rn(-f, __fsub_rn(h, m));
   const float q1 = __fmul_rn(h, r);
   const float rho = __fadd_rn(__fmaf_rn(-q1, e, h), l);
   const float q2 = __fmul_rn(rho, r);
@@ -125,86 +129,176 @@ __device__ __forceinline__ float rd_alpha_ff(float a, float p, float e, float r)
   return rd_alpha_div(h, l, e);
 }
 
-// One sub-ray's walk (radon_rd.c:39-70): visit(pi, pj, l) for every credited
-// step, (pi, pj) the image row and column stepped into, l the length credited.
-template <class Visit>
-__device__ __forceinline__ void rd_walk(const RdGeom &s, int n, int nh, Visit visit) {
+// One sub-ray's walk (radon_rd.c:39-70): visit(ok, off, l) for every step,
+// ok when the pixel stepped into has image row pi and column pj in [1, n-1]
+// (the reference credits only those), off = (pi + pad) sA + (pj + pad) sB its
+// offset in the image the caller reads or writes (sA = row stride, sB = 1
+// row-major; sA = 1, sB = row stride transposed), l the length credited.
+//
+// Two forms.  Checked (Safe): ok as above, and the walk stops after 4n + 16
+// steps: a zero or tiny extent makes that axis' alphas infinite or NaN, on
+// which the reference never ends.  Unchecked (Safe false), for walks with
+// |1/e| <= 2^64 on both axes, where each step raises the stepped axis' next
+// alpha by about 1/|e| (far above the float spacing of alphas <= 1) and no
+// alpha is inf or NaN, so a walk ends after at most |ex| + |ey| + 4 steps;
+// visit gets ok = true for every step:
+// the caller's image then has a frame, rows and columns -1 .. n+1 at
+// pad = 1, holding zeros (reads) or ignored sums (writes) outside
+// [1, n-1]^2.  They are used for walks whose end points all lie within
+// nh + 1/4 of the centre: such a walk stays in rows and columns -1 .. n+1.
+// (x steps, dx = 1: x step j >= 1 happens only if the alpha of x step j - 1
+// was <= 1, i.e. its crossing c <= p1x + ex (1 + 2^-21) <= p2x + 2^-5, so
+// c <= nh - 1/2 and the pixel stepped into, c + 3/2, is <= nh + 1; step 0
+// goes to round(p1x) + 1 <= nh + 1; and round(p1x) >= -nh.  The same for
+// dx = -1 and for y.)
+template <bool Safe, class Visit>
+__device__ __forceinline__ void rd_walk_loop(const RdGeom &s, int n, int nh, int sA, int sB, int pad, float rx,
+                                             float ry, Visit &visit) {
   const float incr = __fsqrt_rn(__fmaf_rn(s.ex, s.ex, __fmul_rn(s.ey, s.ey)));
   const float hx = s.dx > 0 ? 0.5f : -0.5f, hy = s.dy > 0 ? 0.5f : -0.5f;
   const float fdx = hx + hx, fdy = hy + hy;
-  const float rx = __frcp_rn(s.ex), ry = __frcp_rn(s.ey);
-  int ii = s.ii0, jj = s.jj0;
-  // coordinates of the next x and y crossings, stepped exactly by +-1
-  float cx = __fadd_rn((float)s.ii0, hx), cy = __fadd_rn((float)s.jj0, hy);
-  float ax = rd_alpha_ff(cx, s.p1x, s.ex, rx), ay = rd_alpha_ff(cy, s.p1y, s.ey, ry);
+  const float Px = rintf(s.p1x), Py = rintf(s.p1y);
+  const float fx = __fsub_rn(s.p1x, Px), fy = __fsub_rn(s.p1y, Py);
+  // numerators of the next x and y crossings, m - f, m stepped exactly by +-1
+  float mx = __fsub_rn(__fadd_rn((float)s.ii0, hx), Px), my = __fsub_rn(__fadd_rn((float)s.jj0, hy), Py);
+  float ax = rd_alpha_mf(mx, fx, s.ex, rx), ay = rd_alpha_mf(my, fy, s.ey, ry);
+  // the current pixel's row is pi = mx + Px - hx + nh (its next x crossing is
+  // at pi - nh + hx), so pi - n/2 = mx + kx; pi in [1, n-1] iff
+  // |pi - n/2| <= n/2 - 1.  All of it exact in float.
+  const float half = 0.5f * (float)n, lim = half - 1.0f;
+  const float kx = __fsub_rn(__fadd_rn(__fsub_rn(Px, hx), (float)nh), half);
+  const float ky = __fsub_rn(__fadd_rn(__fsub_rn(Py, hy), (float)nh), half);
+  int off = (s.ii0 + nh + pad) * sA + (s.jj0 + nh + pad) * sB;
+  const int ox = s.dx * sA, oy = s.dy * sB;
   float alpha = 0.0f, alpha_old = 0.0f;
-  const int guard = 4 * n + 16;  // a walk crosses at most 2n + 2 lines
-  for (int it = 0; alpha <= 1.0f && it < guard; ++it) {
+  for (int it = Safe ? 4 * n + 16 : 1; alpha <= 1.0f && it > 0; it -= Safe ? 1 : 0) {
     // x step if ax < ay, y step if ax > ay, both if equal (radon_rd.c:45-58);
     // a NaN crossing would never advance the reference: stop.  Written
     // without branches on the step kind, so the lanes of a warp stay together:
     // one new crossing parameter (two on a diagonal step).
     const bool sx = ax <= ay, sy = ay <= ax;
-    if (!(sx || sy)) break;
+    if (Safe && !(sx || sy)) break;
     alpha = sx ? ax : ay;
-    ii += sx ? s.dx : 0;
-    jj += sy ? s.dy : 0;
-    cx = sx ? __fadd_rn(cx, fdx) : cx;
-    cy = sy ? __fadd_rn(cy, fdy) : cy;
-    const float a1 = rd_alpha_ff(sx ? cx : cy, sx ? s.p1x : s.p1y, sx ? s.ex : s.ey, sx ? rx : ry);
+    mx = sx ? __fadd_rn(mx, fdx) : mx;
+    my = sy ? __fadd_rn(my, fdy) : my;
+    off += (sx ? ox : 0) + (sy ? oy : 0);
+    const float a1 = rd_alpha_mf(sx ? mx : my, sx ? fx : fy, sx ? s.ex : s.ey, sx ? rx : ry);
     ax = sx ? a1 : ax;
     ay = sx ? ay : a1;
-    if (sx && sy) ay = rd_alpha_ff(cy, s.p1y, s.ey, ry);
+    if (sx && sy) ay = rd_alpha_mf(my, fy, s.ey, ry);
     const float l = __fmul_rn(__fsub_rn(alpha, alpha_old), incr);
-    const int pi = ii + nh, pj = jj + nh;
-    if ((unsigned)(pi - 1) < (unsigned)(n - 1) && (unsigned)(pj - 1) < (unsigned)(n - 1)) visit(pi, pj, l);
+    visit(!Safe || (fabsf(__fadd_rn(mx, kx)) <= lim && fabsf(__fadd_rn(my, ky)) <= lim), off, l);
     alpha_old = alpha;
   }
 }
 
-__global__ void rd_transpose_kernel(const float *__restrict__ in, float *__restrict__ out, int n) {
+// Whether a walk may run unchecked on a framed image (above): its end points
+// within nh + 1/4 of the centre and |1/e| <= 2^64 on both axes.  Walks that
+// fail it are few: an end point is on the square's edge up to the rounding of
+// the reference's entry / exit arithmetic.
+__device__ __forceinline__ bool rd_walk_framed(const RdGeom &s, int nh, float rx, float ry) {
+  const float reach = fmaxf(fmaxf(fabsf(s.p1x), fabsf(s.p1y)), fmaxf(fabsf(s.p2x), fabsf(s.p2y)));
+  return reach <= (float)nh + 0.25f && fabsf(rx) <= 0x1p64f && fabsf(ry) <= 0x1p64f;
+}
+
+// The forward's credits along walks: acc += 0.2 l x[pixel] in walk order,
+// each credit added one step after its load is issued, so the load is in
+// flight during the next step; a step outside [1, n-1]^2 adds 0 * 0 (checked
+// walks) or w * 0 from the frame (acc is never -0, so that leaves it
+// unchanged).
+struct RdGather {
+  const float *P;
+  float acc, w, xv;
+  __device__ __forceinline__ void operator()(bool ok, int off, float l) {
+    const float x = ok ? __ldg(P + off) : 0.0f;
+    acc = fmaf(w, xv, acc);
+    w = ok ? 0.2f * l : 0.0f;
+    xv = x;
+  }
+};
+
+// The adjoint's credits: fixed_of(0.2 l y) with ys = y 2^E (scaling by a power
+// of two commutes with the rounding of the product).
+struct RdScatter {
+  unsigned long long *P;
+  float ys;
+  __device__ __forceinline__ void operator()(bool ok, int off, float l) {
+    if (ok) atomicAdd(P + off, (unsigned long long)__float2ll_rn(__fmul_rn(0.2f * l, ys)));
+  }
+};
+
+// Checked walks out of line, state passed by value: rarely taken, and kept
+// out of the register budget of the unchecked loop.
+__device__ __noinline__ RdGather rd_walk_safe(RdGeom s, int n, int nh, int sA, int sB, int pad, float rx, float ry,
+                                              RdGather v) {
+  rd_walk_loop<true>(s, n, nh, sA, sB, pad, rx, ry, v);
+  return v;
+}
+
+__device__ __noinline__ void rd_walk_safe(RdGeom s, int n, int nh, int sA, int sB, int pad, float rx, float ry,
+                                          RdScatter v) {
+  rd_walk_loop<true>(s, n, nh, sA, sB, pad, rx, ry, v);
+}
+
+// Framed copies of slice blockIdx.z for the forward's walks: Q (row-major)
+// and QT (transposed), (n + 3)^2 each, Q[(pi + 1)(n + 3) + pj + 1] = x[pi][pj]
+// for pi, pj in [1, n-1] and 0 elsewhere (pi, pj in -1 .. n+1); a 32 x 32
+// tile of the framed grid per block (blockDim 32 x 8).
+__global__ void rd_frame_kernel(const float *__restrict__ in, float *__restrict__ Q, float *__restrict__ QT, int n) {
   __shared__ float tile[32][33];
-  const size_t stride = (size_t)n * n;
-  const float *src = in + (size_t)blockIdx.z * stride;
-  float *dst = out + (size_t)blockIdx.z * stride;
-  const int x = blockIdx.x * 32 + threadIdx.x, y0 = blockIdx.y * 32;
-  for (int dy = threadIdx.y; dy < 32; dy += blockDim.y)
-    if (x < n && y0 + dy < n) tile[dy][threadIdx.x] = src[(size_t)(y0 + dy) * n + x];
+  const int m = n + 3;
+  const float *src = in + (size_t)blockIdx.z * n * n;
+  float *q = Q + (size_t)blockIdx.z * m * m, *qt = QT + (size_t)blockIdx.z * m * m;
+  const int C0 = blockIdx.x * 32, R0 = blockIdx.y * 32;
+  for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+    const int R = R0 + k, C = C0 + threadIdx.x, pi = R - 1, pj = C - 1;
+    const bool in_img = pi >= 1 && pi <= n - 1 && pj >= 1 && pj <= n - 1;
+    const float v = in_img ? src[(size_t)pi * n + pj] : 0.0f;
+    tile[k][threadIdx.x] = v;
+    if (R < m && C < m) q[(size_t)R * m + C] = v;
+  }
   __syncthreads();
-  const int ox = blockIdx.y * 32 + threadIdx.x;
-  for (int dy = threadIdx.y; dy < 32; dy += blockDim.y) {
-    const int oy = blockIdx.x * 32 + dy;
-    if (ox < n && oy < n) dst[(size_t)oy * n + ox] = tile[threadIdx.x][dy];
+  for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+    const int R = C0 + k, C = R0 + threadIdx.x;  // QT[R][C] = Q[C][R]
+    if (R < m && C < m) qt[(size_t)R * m + C] = tile[threadIdx.x][k];
   }
 }
 
-// Forward over slices z0 + blockIdx.z; imgT holds the chunk's slices transposed.
-__global__ void __launch_bounds__(128) rd_forward_kernel(
-    const float *__restrict__ img, const float *__restrict__ imgT, float *__restrict__ sino,
-    const RdAngle *__restrict__ tab, const float *__restrict__ toff, int n, int nh, int na, int z0, FwdEpi ep) {
+// Forward over slices z0 + blockIdx.z; Q and QT hold the chunk's slices
+// framed (rd_frame_kernel).
+__global__ void __launch_bounds__(128, 8) rd_forward_kernel(
+    const float *__restrict__ img, const float *__restrict__ Q, const float *__restrict__ QT,
+    float *__restrict__ sino, const RdAngle *__restrict__ tab, const float *__restrict__ toff, int n, int nh, int na,
+    int z0, FwdEpi ep) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   const int v = blockIdx.y;
   const size_t z = (size_t)z0 + blockIdx.z;
   const bool live = b < n;
   const RdAngle g = tab[v];
-  const float *I = img + z * (size_t)n * n, *IT = imgT + (size_t)blockIdx.z * n * n;
+  const float *I = img + z * (size_t)n * n;
   float acc = 0.0f;
   if (!live) {
   } else if (g.mode == 1) {  // |s| < 1e-7: bin n-1-i <- column i, i >= 1 (radon_rd.c:96-105)
     const int i = n - 1 - b;
     if (i >= 1)
       for (int j = 0; j < n; ++j) acc += __ldg(I + (size_t)j * n + i);
-  } else if (g.mode == 2) {  // |c| < 1e-7: bin i <- row i (:108-117), read down the transposed image
-    for (int j = 0; j < n; ++j) acc += __ldg(IT + (size_t)j * n + b);
+  } else if (g.mode == 2) {  // |c| < 1e-7: bin i <- row i (:108-117)
+    for (int j = 0; j < n; ++j) acc += __ldg(I + (size_t)b * n + j);
   } else {
+    const int m = n + 3;
     const bool tr = g.tr != 0;
-    const float *P = tr ? IT : I;
+    const float *P = (tr ? QT : Q) + (size_t)blockIdx.z * m * m;
+    const int sA = tr ? 1 : m, sB = tr ? m : 1;
+    RdGather v{P, 0.0f, 0.0f, 0.0f};
     for (int r = 1; r <= 5; ++r) {
       const RdGeom s = rd_geom(rd_offset_tab(toff, 6 * b + r, n, g.lt, g.gt), g, nh);
-      rd_walk(s, n, nh, [&](int pi, int pj, float l) {
-        acc = fmaf(0.2f * l, __ldg(P + (tr ? (size_t)pj * n + pi : (size_t)pi * n + pj)), acc);
-      });
+      const float rx = __frcp_rn(s.ex), ry = __frcp_rn(s.ey);
+      if (rd_walk_framed(s, nh, rx, ry))
+        rd_walk_loop<false>(s, n, nh, sA, sB, 1, rx, ry, v);
+      else
+        v = rd_walk_safe(s, n, nh, sA, sB, 1, rx, ry, v);
     }
+    acc = fmaf(v.w, v.xv, v.acc);
   }
   // store through the epilogue; residual slot as in one launch over all slices
   const size_t e = (z * na + v) * (size_t)n + (live ? b : 0);
@@ -234,7 +328,10 @@ __device__ __noinline__ void rd_scatter_nonfinite(float y, const RdAngle *__rest
   } else {
     for (int r = 1; r <= 5; ++r) {
       const RdGeom s = rd_geom(rd_offset_tab(toff, 6 * b + r, n, g.lt, g.gt), g, nh);
-      rd_walk(s, n, nh, [&](int pi, int pj, float l) { rd_flag(Fl, (size_t)pi * n + pj, __fmul_rn(0.2f * l, y)); });
+      auto flag = [&](bool ok, int off, float l) {
+        if (ok) rd_flag(Fl, (size_t)off, __fmul_rn(0.2f * l, y));
+      };
+      rd_walk_loop<true>(s, n, nh, n, 1, 0, __frcp_rn(s.ex), __frcp_rn(s.ey), flag);
     }
   }
 }
@@ -247,12 +344,16 @@ __device__ __forceinline__ FixedScale rd_adj_scale(const unsigned *smax, int na)
   return fixed_scale(4.0 * (double)na * (double)__uint_as_float(*smax));
 }
 
-// Adjoint scatter: slice blockIdx.z of the chunk; accf its fixed-point image,
-// accT the transposed one that angles with |s| > |c| add into.
+// Adjoint scatter: slice blockIdx.z of the chunk.  Walk credits go to the
+// framed fixed-point images F (row-major) and FT (transposed, for angles with
+// |s| > |c|), (n + 3)^2 each, pixel (pi, pj) at (pi + 1)(n + 3) + pj + 1; the
+// frame and row / column 0 collect credits the reference does not make, which
+// the finalize ignores.  The row / column-sum angles add their one credit per
+// pixel to per-column (cols) and per-row (rows) sums instead.
 __global__ void __launch_bounds__(128) rd_scatter_kernel(
     const float *__restrict__ sino, unsigned long long *__restrict__ accf, unsigned long long *__restrict__ accT,
-    unsigned *__restrict__ flags, const RdAngle *__restrict__ tab, const float *__restrict__ toff, int n, int nh,
-    int na, const unsigned *__restrict__ smax) {
+    unsigned long long *__restrict__ lines, unsigned *__restrict__ flags, const RdAngle *__restrict__ tab,
+    const float *__restrict__ toff, int n, int nh, int na, const unsigned *__restrict__ smax) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   const int v = blockIdx.y;
   const size_t z = blockIdx.z;
@@ -265,46 +366,48 @@ __global__ void __launch_bounds__(128) rd_scatter_kernel(
     return;
   }
   const FixedScale fs = rd_adj_scale(smax + z, na);
-  unsigned long long *F = accf + z * (size_t)n * n, *FT = accT + z * (size_t)n * n;
+  const int m = n + 3;
+  unsigned long long *cols = lines + z * 2 * (size_t)n, *rows = cols + n;
   if (g.mode == 1) {  // column n-1-b, every row (transpose of radon_rd.c:96-105)
     const int i = n - 1 - b;
-    if (i >= 1) {
-      const unsigned long long q = fixed_of(y, fs);
-      for (int j = 0; j < n; ++j) atomicAdd(F + (size_t)j * n + i, q);
-    }
+    if (i >= 1) atomicAdd(cols + i, fixed_of(y, fs));
     return;
   }
-  if (g.mode == 2) {  // row b, every column (:108-117), down the transposed image
-    const unsigned long long q = fixed_of(y, fs);
-    for (int j = 0; j < n; ++j) atomicAdd(FT + (size_t)j * n + b, q);
+  if (g.mode == 2) {  // row b, every column (:108-117)
+    atomicAdd(rows + b, fixed_of(y, fs));
     return;
   }
   const bool tr = g.tr != 0;
-  unsigned long long *P = tr ? FT : F;
-  // y 2^E: scaling by a power of two commutes with the rounding of the
-  // product, so each credit is fixed_of(0.2 l y) with one multiply fewer
-  const float ys = __fmul_rn(__fmul_rn(y, fs.s1), fs.s2);
+  unsigned long long *P = (tr ? accT : accf) + z * (size_t)m * m;
+  const int sA = tr ? 1 : m, sB = tr ? m : 1;
+  RdScatter add{P, __fmul_rn(__fmul_rn(y, fs.s1), fs.s2)};
   for (int r = 1; r <= 5; ++r) {
     const RdGeom s = rd_geom(rd_offset_tab(toff, 6 * b + r, n, g.lt, g.gt), g, nh);
-    rd_walk(s, n, nh, [&](int pi, int pj, float l) {
-      atomicAdd(P + (tr ? (size_t)pj * n + pi : (size_t)pi * n + pj),
-                (unsigned long long)__float2ll_rn(__fmul_rn(0.2f * l, ys)));
-    });
+    const float rx = __frcp_rn(s.ex), ry = __frcp_rn(s.ey);
+    if (rd_walk_framed(s, nh, rx, ry))
+      rd_walk_loop<false>(s, n, nh, sA, sB, 1, rx, ry, add);
+    else
+      rd_walk_safe(s, n, nh, sA, sB, 1, rx, ry, add);
   }
 }
 
-// accf + accT transposed -> float through the adjoint epilogue, a 32 x 32 tile
-// per block (blockDim 32 x 8); slice blockIdx.z of the chunk is slice z0 + it.
+// Walk credits of pixels in [1, n-1]^2 (F + FT transposed) plus the row and
+// column sums -> float through the adjoint epilogue, a 32 x 32 tile per block
+// (blockDim 32 x 8); slice blockIdx.z of the chunk is slice z0 + it.
 __global__ void rd_finalize_kernel(const unsigned long long *__restrict__ accf,
-                                   const unsigned long long *__restrict__ accT, const unsigned *__restrict__ flags,
+                                   const unsigned long long *__restrict__ accT,
+                                   const unsigned long long *__restrict__ lines, const unsigned *__restrict__ flags,
                                    float *__restrict__ img, int n, int z0, int na, const unsigned *__restrict__ smax,
                                    AdjEpi ep) {
   __shared__ unsigned long long tile[32][33];
   const size_t zl = blockIdx.z, per = (size_t)n * n;
-  const unsigned long long *F = accf + zl * per, *FT = accT + zl * per;
+  const int m = n + 3;
+  const unsigned long long *F = accf + zl * (size_t)m * m, *FT = accT + zl * (size_t)m * m;
+  const unsigned long long *cols = lines + zl * 2 * (size_t)n, *rows = cols + n;
   const int R0 = blockIdx.y * 32, C0 = blockIdx.x * 32;
-  for (int k = threadIdx.y; k < 32; k += blockDim.y)  // tile[c][r] = accT[(C0 + c) n + R0 + r]
-    if (C0 + k < n && R0 + threadIdx.x < n) tile[k][threadIdx.x] = FT[(size_t)(C0 + k) * n + R0 + threadIdx.x];
+  for (int k = threadIdx.y; k < 32; k += blockDim.y)  // tile[c][r] = FT at pixel (R0 + r, C0 + c)
+    if (C0 + k < n && R0 + threadIdx.x < n)
+      tile[k][threadIdx.x] = FT[(size_t)(C0 + k + 1) * m + R0 + threadIdx.x + 1];
   __syncthreads();
   const FixedScale fs = rd_adj_scale(smax + zl, na);
   for (int k = threadIdx.y; k < 32; k += blockDim.y) {
@@ -314,19 +417,23 @@ __global__ void rd_finalize_kernel(const unsigned long long *__restrict__ accf,
     if (live) {
       const size_t p = (size_t)R * n + C;
       const unsigned f = (flags[zl * ((per + 3) / 4) + (p >> 2)] >> (8u * (unsigned)(p & 3))) & 0xffu;
-      val = f == 0u ? fixed_to_float(F[p] + tile[threadIdx.x][k], fs) : nonfinite_value(f);
+      unsigned long long q = cols[C] + rows[R];
+      if (R >= 1 && C >= 1) q += F[(size_t)(R + 1) * m + C + 1] + tile[threadIdx.x][k];
+      val = f == 0u ? fixed_to_float(q, fs) : nonfinite_value(f);
     }
     adj_store(ep, val, live, ((size_t)z0 + zl) * per + (live ? (size_t)R * n + C : 0), img);
   }
 }
 
-// slices per chunk: the adjoint's two fixed-point images and flag bytes (the
-// forward's transposed image uses the same space) of at most 512 MiB, and no
-// more than a grid dimension holds
+// slices per chunk: the adjoint's two framed fixed-point images, row and
+// column sums and flag bytes (the forward's framed images use the same space)
+// of at most 512 MiB, and no more than a grid dimension holds
 size_t rd_flag_words(const Plan &p) { return ((size_t)p.g.n * p.g.n + 3) / 4; }
 
+size_t rd_framed(const Plan &p) { return (size_t)(p.g.n + 3) * (p.g.n + 3); }
+
 int rd_chunk(const Plan &p) {
-  const size_t per = (size_t)16 * p.g.n * p.g.n + 4 * rd_flag_words(p);
+  const size_t per = 16 * rd_framed(p) + 16 * (size_t)p.g.n + 4 * rd_flag_words(p);
   const size_t cap = std::min<size_t>(((size_t)512 << 20) / per, 65535);
   return (int)std::max<size_t>(1, std::min<size_t>((size_t)p.g.nz, cap));
 }
@@ -363,23 +470,24 @@ int rd_setup(Plan &p) {
   TOMO_CUDA(cudaMemcpy(p.d_angles, tab.data(), sizeof(RdAngle) * (size_t)na, cudaMemcpyHostToDevice));
   TOMO_CUDA(cudaMalloc(&p.d_aux, sizeof(float) * toff.size()));
   TOMO_CUDA(cudaMemcpy(p.d_aux, toff.data(), sizeof(float) * toff.size(), cudaMemcpyHostToDevice));
-  // scratch: a chunk of fixed-point images, of transposed ones and of flag
-  // bytes (the forward's transposed images in the same space), then max |y|
-  // per slice
-  p.scratch_bytes = ((size_t)16 * n * n + 4 * rd_flag_words(p)) * rd_chunk(p) + sizeof(unsigned) * (size_t)p.g.nz;
+  // scratch: a chunk of framed fixed-point images, of transposed ones, of row
+  // and column sums and of flag bytes (the forward's framed images in the
+  // same space), then max |y| per slice
+  p.scratch_bytes = (16 * rd_framed(p) + 16 * (size_t)n + 4 * rd_flag_words(p)) * rd_chunk(p) +
+                    sizeof(unsigned) * (size_t)p.g.nz;
   TOMO_CUDA(cudaMalloc(&p.d_scratch, p.scratch_bytes));
   return TOMO_OK;
 }
 
 int rd_forward(Plan &p, const float *d_img, float *d_sino, cudaStream_t s, const FwdEpi &ep) {
-  const int n = p.g.n, na = p.g.na, nz = p.g.nz, chunk = rd_chunk(p);
-  float *imgT = p.d_scratch;
+  const int n = p.g.n, na = p.g.na, nz = p.g.nz, chunk = rd_chunk(p), m = n + 3;
+  float *Q = p.d_scratch, *QT = Q + (size_t)chunk * rd_framed(p);
   for (int z0 = 0; z0 < nz; z0 += chunk) {
     const int zc = std::min(chunk, nz - z0);
-    rd_transpose_kernel<<<dim3((n + 31) / 32, (n + 31) / 32, zc), dim3(32, 8), 0, s>>>(
-        d_img + (size_t)z0 * n * n, imgT, n);
+    rd_frame_kernel<<<dim3((m + 31) / 32, (m + 31) / 32, zc), dim3(32, 8), 0, s>>>(d_img + (size_t)z0 * n * n, Q,
+                                                                                     QT, n);
     rd_forward_kernel<<<dim3((n + 127) / 128, na, zc), 128, 0, s>>>(
-        d_img, imgT, d_sino, (const RdAngle *)p.d_angles, (const float *)p.d_aux, n, p.nh, na, z0, ep);
+        d_img, Q, QT, d_sino, (const RdAngle *)p.d_angles, (const float *)p.d_aux, n, p.nh, na, z0, ep);
   }
   TOMO_CUDA(cudaGetLastError());
   return TOMO_OK;
@@ -387,24 +495,27 @@ int rd_forward(Plan &p, const float *d_img, float *d_sino, cudaStream_t s, const
 
 int rd_adjoint(Plan &p, const float *d_sino, float *d_img, cudaStream_t s, const AdjEpi &ep) {
   const int n = p.g.n, na = p.g.na, nz = p.g.nz, chunk = rd_chunk(p);
-  const size_t per_img = (size_t)n * n, per_sino = (size_t)na * n;
+  const size_t per_sino = (size_t)na * n;
+  const size_t per_fr = rd_framed(p);
   unsigned long long *accf = reinterpret_cast<unsigned long long *>(p.d_scratch);
-  unsigned long long *accT = accf + (size_t)chunk * per_img;
+  unsigned long long *accT = accf + (size_t)chunk * per_fr;
+  unsigned long long *lines = accT + (size_t)chunk * per_fr;
   const size_t fw = rd_flag_words(p);
-  unsigned *flags = reinterpret_cast<unsigned *>(accT + (size_t)chunk * per_img);
+  unsigned *flags = reinterpret_cast<unsigned *>(lines + (size_t)chunk * 2 * n);
   unsigned *smax = flags + (size_t)chunk * fw;
   TOMO_CUDA(cudaMemsetAsync(smax, 0, sizeof(unsigned) * (size_t)nz, s));
   for (int z0 = 0; z0 < nz; z0 += chunk) {
     const int zc = std::min(chunk, nz - z0);
     fixed_finite_absmax_kernel<<<dim3(64, zc), 256, 0, s>>>(d_sino + (size_t)z0 * per_sino, per_sino, smax + z0);
-    TOMO_CUDA(cudaMemsetAsync(accf, 0, sizeof(unsigned long long) * zc * per_img, s));
-    TOMO_CUDA(cudaMemsetAsync(accT, 0, sizeof(unsigned long long) * zc * per_img, s));
+    TOMO_CUDA(cudaMemsetAsync(accf, 0, sizeof(unsigned long long) * zc * per_fr, s));
+    TOMO_CUDA(cudaMemsetAsync(accT, 0, sizeof(unsigned long long) * zc * per_fr, s));
+    TOMO_CUDA(cudaMemsetAsync(lines, 0, sizeof(unsigned long long) * zc * 2 * (size_t)n, s));
     TOMO_CUDA(cudaMemsetAsync(flags, 0, sizeof(unsigned) * zc * fw, s));
     rd_scatter_kernel<<<dim3((n + 127) / 128, na, zc), 128, 0, s>>>(
-        d_sino + (size_t)z0 * per_sino, accf, accT, flags, (const RdAngle *)p.d_angles, (const float *)p.d_aux, n,
-        p.nh, na, smax + z0);
+        d_sino + (size_t)z0 * per_sino, accf, accT, lines, flags, (const RdAngle *)p.d_angles,
+        (const float *)p.d_aux, n, p.nh, na, smax + z0);
     rd_finalize_kernel<<<dim3((n + 31) / 32, (n + 31) / 32, zc), dim3(32, 8), 0, s>>>(
-        accf, accT, flags, d_img, n, z0, na, smax + z0, ep);
+        accf, accT, lines, flags, d_img, n, z0, na, smax + z0, ep);
   }
   TOMO_CUDA(cudaGetLastError());
   return TOMO_OK;

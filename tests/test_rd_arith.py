@@ -1,5 +1,5 @@
-"""CPU checks of the float-only arithmetic in the ray-driven adjoint
-(csrc/radon_rd.cu: rd_alpha_ff, rd_alpha_approx, rd_round_i).
+"""CPU checks of the float-only arithmetic of the ray-driven walk
+(csrc/radon_rd.cu: rd_alpha_mf, rd_walk_loop's pixel range test, rd_round_i).
 
 The reference computes each crossing parameter as a double quotient rounded to
 float, alpha = (float)(((double)a - p) / (p2 - p1)) (radon_rd.c:41-42), and the
@@ -26,14 +26,30 @@ def _rn(x):
     return np.asarray(x, dtype=f32)
 
 
+def two_sum(a, p):
+    """Knuth's TwoSum of a and -p: h + l == a - p exactly."""
+    h = a - p
+    bb = h - a
+    return h, (a - (h - bb)) + (-p - bb)
+
+
+def split_numerator(a, p):
+    """The walk's numerator a - p as m - f: P = rint(p), f = p - P, m = a - P
+    (rd_walk_loop), then Fast2Sum (rd_alpha_mf): h + l == m - f."""
+    P = np.rint(p)
+    f = p - P
+    m = a - P
+    h = m - f
+    l = -f - (h - m)
+    return m, f, h, l
+
+
 def alpha_ff(a, p, e):
-    """rd_alpha_ff's fast path: (value, accepted)."""
+    """rd_alpha_mf's fast path on the numerator a - p: (value, accepted)."""
     a, p, e = _rn(a), _rn(p), _rn(e)
     with np.errstate(all="ignore"):
         r = f32(1.0) / e                              # __frcp_rn
-        h = a - p
-        bb = h - a
-        l = (a - (h - bb)) + (-p - bb)                # TwoSum: h + l == a - p
+        _, _, h, l = split_numerator(a, p)
         q1 = h * r
         fma = (-(q1.astype(np.longdouble)) * e.astype(np.longdouble) + h.astype(np.longdouble)).astype(f32)
         rho = fma + l
@@ -142,3 +158,43 @@ def test_round_half_away_by_round_down_adds():
     got = np.where(x < 0, -got, got)
     ref = (np.sign(x.astype(f64)) * np.floor(np.abs(x.astype(f64)) + 0.5)).astype(np.int64)
     assert np.array_equal(got, ref)
+
+
+@pytest.mark.parametrize("seed", [0, 1])
+def test_split_numerator_is_exact(seed):
+    """m and f are exact, and Fast2Sum of (m, -f) gives TwoSum's (h, l) of
+    (a, -p): the same float pair, so the same quotient and the same fallback."""
+    rng = np.random.default_rng(100 + seed)
+    a, p, _ = _random_inputs(rng, 2_000_000)
+    m, f, h, l = split_numerator(a, p)
+    P = np.rint(p).astype(f64)
+    assert np.array_equal(f.astype(f64), p.astype(f64) - P)
+    assert np.array_equal(m.astype(f64), a.astype(f64) - P)
+    assert np.all(np.abs(m) >= 0.5) and np.all(np.abs(f) <= 0.5)
+    h2, l2 = two_sum(a, p)
+    assert np.array_equal(h.view(np.uint32), h2.view(np.uint32))
+    assert np.array_equal(l, l2)    # equal as values (+0 and -0 alike)
+    # and stepping m by +-1 keeps it exact: m - f stays a - p
+    for k in (1, 7, 900):
+        mk = m + f32(k)
+        assert np.array_equal(mk.astype(f64), (a + f32(k)).astype(f64) - P)
+
+
+@pytest.mark.parametrize("n", [2, 3, 64, 255, 256, 2048, 2049])
+def test_pixel_range_test(n):
+    """rd_walk_loop's |mx + kx| <= n/2 - 1 is the reference's
+    0 < ii + nh < n, for every pixel a walk can reach and both directions."""
+    rng = np.random.default_rng(n)
+    nh = n // 2
+    half = f32(0.5) * f32(n)
+    lim = half - f32(1)
+    for hx in (f32(0.5), f32(-0.5)):
+        p1 = rng.uniform(-nh - 3, nh + 3, 4000).astype(f32)
+        P = np.rint(p1)
+        ii = np.arange(-nh - 8, nh + 9)
+        II, PP = np.meshgrid(ii, P)
+        mx = (II.astype(f32) + hx) - PP                 # the next x crossing's m
+        kx = ((PP - hx) + f32(nh)) - half
+        got = np.abs(mx + kx) <= lim
+        pi = II + nh
+        assert np.array_equal(got, (pi > 0) & (pi < n))
