@@ -265,13 +265,18 @@ __global__ void rd_frame_kernel(const float *__restrict__ in, float *__restrict_
 }
 
 // Forward over slices z0 + blockIdx.z; Q and QT hold the chunk's slices
-// framed (rd_frame_kernel).
-__global__ void __launch_bounds__(128, 8) rd_forward_kernel(
+// framed (rd_frame_kernel).  A block is 128 bins of kFwdAngles consecutive
+// angles (threadIdx.y): the walks of neighbouring angles cover nearly the same
+// pixels at nearly the same time, so its warps share L1 lines.
+constexpr int kFwdAngles = 4;
+
+__global__ void __launch_bounds__(128 * kFwdAngles, 8 / kFwdAngles) rd_forward_kernel(
     const float *__restrict__ img, const float *__restrict__ Q, const float *__restrict__ QT,
     float *__restrict__ sino, const RdAngle *__restrict__ tab, const float *__restrict__ toff, int n, int nh, int na,
     int z0, FwdEpi ep) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
-  const int v = blockIdx.y;
+  const int v = blockIdx.y * kFwdAngles + threadIdx.y;
+  if (v >= na) return;  // whole warps
   const size_t z = (size_t)z0 + blockIdx.z;
   const bool live = b < n;
   const RdAngle g = tab[v];
@@ -289,22 +294,22 @@ __global__ void __launch_bounds__(128, 8) rd_forward_kernel(
     const bool tr = g.tr != 0;
     const float *P = (tr ? QT : Q) + (size_t)blockIdx.z * m * m;
     const int sA = tr ? 1 : m, sB = tr ? m : 1;
-    RdGather v{P, 0.0f, 0.0f, 0.0f};
+    RdGather gat{P, 0.0f, 0.0f, 0.0f};
     for (int r = 1; r <= 5; ++r) {
       const RdGeom s = rd_geom(rd_offset_tab(toff, 6 * b + r, n, g.lt, g.gt), g, nh);
       const float rx = __frcp_rn(s.ex), ry = __frcp_rn(s.ey);
       if (rd_walk_framed(s, nh, rx, ry))
-        rd_walk_loop<false>(s, n, nh, sA, sB, 1, rx, ry, v);
+        rd_walk_loop<false>(s, n, nh, sA, sB, 1, rx, ry, gat);
       else
-        v = rd_walk_safe(s, n, nh, sA, sB, 1, rx, ry, v);
+        gat = rd_walk_safe(s, n, nh, sA, sB, 1, rx, ry, gat);
     }
-    acc = fmaf(v.w, v.xv, v.acc);
+    acc = fmaf(gat.w, gat.xv, gat.acc);
   }
   // store through the epilogue; residual slot as in one launch over all slices
   const size_t e = (z * na + v) * (size_t)n + (live ? b : 0);
   double r2 = 0.0;
   if (live) sino[e] = fwd_apply(ep, acc, e, r2);
-  fwd_resid_commit(ep, r2, ((z * gridDim.y + v) * gridDim.x + blockIdx.x) * (blockDim.x / 32) + threadIdx.x / 32);
+  fwd_resid_commit(ep, r2, ((z * na + v) * gridDim.x + blockIdx.x) * (blockDim.x / 32) + threadIdx.x / 32);
 }
 
 // Flag bytes of non-finite credits (nonfinite_flag: 1 +inf, 2 -inf, 4 NaN),
@@ -486,7 +491,7 @@ int rd_forward(Plan &p, const float *d_img, float *d_sino, cudaStream_t s, const
     const int zc = std::min(chunk, nz - z0);
     rd_frame_kernel<<<dim3((m + 31) / 32, (m + 31) / 32, zc), dim3(32, 8), 0, s>>>(d_img + (size_t)z0 * n * n, Q,
                                                                                      QT, n);
-    rd_forward_kernel<<<dim3((n + 127) / 128, na, zc), 128, 0, s>>>(
+    rd_forward_kernel<<<dim3((n + 127) / 128, (na + kFwdAngles - 1) / kFwdAngles, zc), dim3(128, kFwdAngles), 0, s>>>(
         d_img, Q, QT, d_sino, (const RdAngle *)p.d_angles, (const float *)p.d_aux, n, p.nh, na, z0, ep);
   }
   TOMO_CUDA(cudaGetLastError());
