@@ -94,6 +94,14 @@ __device__ __forceinline__ RdGeom rd_geom(float t, const RdAngle &g, int nh) {
   return r;
 }
 
+// Geometry of sub-ray i of angle v, out of line: the angle's table entry is
+// read here, so the walks' callers do not hold it across the walks.
+__device__ __noinline__ RdGeom rd_geom_of(const RdAngle *__restrict__ tab, int v, const float *__restrict__ toff,
+                                          int i, int n, int nh) {
+  const RdAngle g = tab[v];
+  return rd_geom(rd_offset_tab(toff, i, n, g.lt, g.gt), g, nh);
+}
+
 // The double division of rd_alpha_mf, out of line: rarely taken, and its
 // double registers stay out of the walk loops.
 __device__ __noinline__ float rd_alpha_div(float h, float l, float e) {
@@ -301,7 +309,7 @@ __global__ void __launch_bounds__(128 * kFwdAngles, 8 / kFwdAngles) rd_forward_k
     const int sA = tr ? 1 : m, sB = tr ? m : 1;
     RdGather gat{P, 0.0f, 0.0f, 0.0f};
     for (int r = 1; r <= 5; ++r) {
-      const RdGeom s = rd_geom(rd_offset_tab(toff, 6 * b + r, n, g.lt, g.gt), g, nh);
+      const RdGeom s = rd_geom_of(tab, v, toff, 6 * b + r, n, nh);
       const float rx = __frcp_rn(s.ex), ry = __frcp_rn(s.ey);
       if (rd_walk_framed(s, nh, rx, ry))
         rd_walk_loop<false>(s, n, nh, sA, sB, 1, rx, ry, gat);
@@ -392,7 +400,7 @@ __global__ void __launch_bounds__(128) rd_scatter_kernel(
   const int sA = tr ? 1 : m, sB = tr ? m : 1;
   RdScatter add{P, __fmul_rn(__fmul_rn(y, fs.s1), fs.s2)};
   for (int r = 1; r <= 5; ++r) {
-    const RdGeom s = rd_geom(rd_offset_tab(toff, 6 * b + r, n, g.lt, g.gt), g, nh);
+    const RdGeom s = rd_geom_of(tab, v, toff, 6 * b + r, n, nh);
     const float rx = __frcp_rn(s.ex), ry = __frcp_rn(s.ey);
     if (rd_walk_framed(s, nh, rx, ry))
       rd_walk_loop<false>(s, n, nh, sA, sB, 1, rx, ry, add);
