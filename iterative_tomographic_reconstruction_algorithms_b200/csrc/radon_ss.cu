@@ -78,25 +78,74 @@ __global__ void __launch_bounds__(128) ss_forward_kernel(
   fwd_store(ep, acc, live, z * (size_t)na * n + (size_t)g.out_row * n + (live ? kt : 0), sino);
 }
 
-// Adjoint: one thread per output pixel, all angles in order.  For the pixel
-// (row R, column C) and an angle, the rays that touch it are those whose
-// minor coordinate lands in [C' - 1, C' + 1) at the pixel's major coordinate;
-// at most 3 candidate t per angle are checked with the forward arithmetic.
+// Adjoint: a thread holds 4 x 4 output pixels (rows R0..R0+3, columns
+// C0..C0+3), all angles in order.  For an angle the pixels fall into 4
+// groups of 4 along the minor axis (a row of the block for steep angles, a
+// column otherwise); the rays that touch a pixel are those whose minor
+// coordinate lands in [minor - 1, minor + 1) at the pixel's major coordinate,
+// so a group's candidate rays are the integers t of one short interval (at
+// most 7: |rb| >= 1), each checked once with the forward arithmetic and
+// credited to the one or two pixels of the group it reaches.  Each pixel gets
+// the credits of its rays in the order t ascending, angle after angle, as a
+// thread per pixel would give them.
 constexpr int kSsChunk = 512;
+constexpr int kSsPix = 4;  // pixels per thread along each axis
+
+// The credits of angle g to the group of pixels with major coordinate m and
+// minor indices minor0 .. minor0 + 3 (a0 .. a3 the pixels at minor0 + 0 .. 3).
+__device__ __forceinline__ void ss_adj_group(const SsAngle &g, float cb, int m, int minor0, int nh,
+                                             const float *__restrict__ row, const int2 *__restrict__ lrow,
+                                             float &a0, float &a1, float &a2, float &a3) {
+  // f(t) = fma(-m, a, t) * rb ~ (t - m a) rb must land in [minor0 - nh - 1,
+  // minor0 + 3 - nh + 1): t in [ta, tb] up to rounding (below 1e-3 here), so
+  // the integers in [ta - 0.01, tb + 0.01] are the candidates
+  const float ma = (float)m * g.a;
+  const float lo = (float)(minor0 - nh - 1), hi = (float)(minor0 + kSsPix - nh);
+  float ta = fmaf(lo, cb, ma), tb = fmaf(hi, cb, ma);
+  if (ta > tb) {
+    const float x = ta;
+    ta = tb;
+    tb = x;
+  }
+  float fl0, fl1;
+  const int t0 = max(floor_i(ta - 0.01f, fl0) + 1, -nh), t1 = min(floor_i(tb + 0.01f, fl1), nh - 1);
+  for (int t = t0; t <= t1; ++t) {
+    const int2 L = __ldg(lrow + t + nh);
+    if (m < L.x || m >= L.y) continue;
+    const float f = __fmul_rn(__fmaf_rn(-(float)m, g.a, (float)t), g.rb);
+    float fl;
+    const int d = floor_i(f, fl) + nh - minor0;  // the ray's left pixel, relative to minor0
+    if (d < -1 || d >= kSsPix) continue;
+    const float y = __ldg(row + t + nh);
+    const float c1 = __fmul_rn(g.wt, __fsub_rn(__fadd_rn(fl, 1.0f), f));  // to pixel d
+    const float c0 = __fmul_rn(g.wt, __fsub_rn(f, fl));                     // to pixel d + 1
+    if (d == 0) a0 = fmaf(c1, y, a0);
+    if (d == -1) a0 = fmaf(c0, y, a0);
+    if (d == 1) a1 = fmaf(c1, y, a1);
+    if (d == 0) a1 = fmaf(c0, y, a1);
+    if (d == 2) a2 = fmaf(c1, y, a2);
+    if (d == 1) a2 = fmaf(c0, y, a2);
+    if (d == 3) a3 = fmaf(c1, y, a3);
+    if (d == 2) a3 = fmaf(c0, y, a3);
+  }
+}
 
 __global__ void __launch_bounds__(256) ss_adjoint_kernel(
     const float *__restrict__ sino, float *__restrict__ img, const SsAngle *__restrict__ tab,
     const int2 *__restrict__ lim, int n, int nh, int na, AdjEpi ep) {
   __shared__ SsAngle stab[kSsChunk];
   __shared__ float cbs[kSsChunk];  // 1 / rb (cos or sin)
-  const int C = blockIdx.x * blockDim.x + threadIdx.x;
-  const int R = blockIdx.y * blockDim.y + threadIdx.y;
+  const int C0 = (blockIdx.x * blockDim.x + threadIdx.x) * kSsPix;
+  const int R0 = (blockIdx.y * blockDim.y + threadIdx.y) * kSsPix;
   const size_t z = blockIdx.z;
-  const bool live = R < n && C < n;
   const float *S = sino + z * (size_t)na * n;
   const int tid = threadIdx.y * blockDim.x + threadIdx.x, nthr = blockDim.x * blockDim.y;
   const int nt = 2 * nh;
-  float acc = 0.0f;
+  float acc[kSsPix][kSsPix];
+#pragma unroll
+  for (int i = 0; i < kSsPix; ++i)
+#pragma unroll
+    for (int j = 0; j < kSsPix; ++j) acc[i][j] = 0.0f;
   for (int v0 = 0; v0 < na; v0 += kSsChunk) {
     const int cnt = min(kSsChunk, na - v0);
     __syncthreads();
@@ -105,41 +154,32 @@ __global__ void __launch_bounds__(256) ss_adjoint_kernel(
       cbs[t] = 1.0f / tab[v0 + t].rb;
     }
     __syncthreads();
-    if (!live) continue;
+    if (R0 >= n || C0 >= n) continue;
     for (int u = 0; u < cnt; ++u) {
       const SsAngle g = stab[u];
+      const float cb = cbs[u];
       const int v = v0 + u;
-      // major coordinate m and minor index of this pixel
-      const int m = g.steep ? R - nh : C - nh;
-      const int minor = g.steep ? C : R;
-      // f(t) = fma(-m, a, t) * rb ~ (t - m a) rb must land in [minor-nh-1, minor-nh+1):
-      // t in [ta, tb] up to rounding (below 1e-3 here), so the integers in
-      // [ta - 0.01, tb + 0.01] are the candidates (at most 3: |rb| >= 1)
-      const float ma = (float)m * g.a;
-      const float lo = (float)(minor - nh - 1), hi = (float)(minor - nh + 1);
-      float ta = fmaf(lo, cbs[u], ma), tb = fmaf(hi, cbs[u], ma);
-      if (ta > tb) { float x = ta; ta = tb; tb = x; }
-      float fl0, fl1;
-      int t0 = floor_i(ta - 0.01f, fl0) + 1, t1 = floor_i(tb + 0.01f, fl1);
-      t0 = max(t0, -nh);
-      t1 = min(t1, nh - 1);
       const float *row = S + (size_t)g.out_row * n;
       const int2 *lrow = lim + (size_t)v * nt;
-      for (int t = t0; t <= t1; ++t) {
-        const int2 L = __ldg(lrow + t + nh);
-        if (m < L.x || m >= L.y) continue;
-        const float f = __fmul_rn(__fmaf_rn(-(float)m, g.a, (float)t), g.rb);
-        float fl;
-        const int q = floor_i(f, fl) + nh;
-        float wgt;
-        if (q == minor) wgt = __fsub_rn(__fadd_rn(fl, 1.0f), f);
-        else if (q + 1 == minor) wgt = __fsub_rn(f, fl);
-        else continue;
-        acc = fmaf(g.wt * wgt, __ldg(row + t + nh), acc);
+      if (g.steep) {  // major axis y: row R is m = R - nh, minor = column
+#pragma unroll
+        for (int i = 0; i < kSsPix; ++i)
+          ss_adj_group(g, cb, R0 + i - nh, C0, nh, row, lrow, acc[i][0], acc[i][1], acc[i][2], acc[i][3]);
+      } else {  // major axis x: column C is m = C - nh, minor = row
+#pragma unroll
+        for (int j = 0; j < kSsPix; ++j)
+          ss_adj_group(g, cb, C0 + j - nh, R0, nh, row, lrow, acc[0][j], acc[1][j], acc[2][j], acc[3][j]);
       }
     }
   }
-  adj_store(ep, acc, live, z * (size_t)n * n + (size_t)(live ? R : 0) * n + (live ? C : 0), img);
+#pragma unroll
+  for (int i = 0; i < kSsPix; ++i)
+#pragma unroll
+    for (int j = 0; j < kSsPix; ++j) {
+      const int R = R0 + i, C = C0 + j;
+      const bool live = R < n && C < n;
+      adj_store(ep, acc[i][j], live, z * (size_t)n * n + (live ? (size_t)R * n + C : 0), img);
+    }
 }
 
 static void sort4(float *a) {
@@ -206,7 +246,7 @@ int ss_forward(Plan &p, const float *d_img, float *d_sino, cudaStream_t s, const
 
 int ss_adjoint(Plan &p, const float *d_sino, float *d_img, cudaStream_t s, const AdjEpi &ep) {
   const int n = p.g.n, na = p.g.na, nz = p.g.nz;
-  dim3 ab(32, 8), ag((n + 31) / 32, (n + 7) / 8, nz);
+  dim3 ab(32, 8), ag((n + 32 * kSsPix - 1) / (32 * kSsPix), (n + 8 * kSsPix - 1) / (8 * kSsPix), nz);
   ss_adjoint_kernel<<<ag, ab, 0, s>>>(d_sino, d_img, (const SsAngle *)p.d_angles,
                                       (const int2 *)p.d_aux, n, p.nh, na, ep);
   TOMO_CUDA(cudaGetLastError());
