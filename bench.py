@@ -408,6 +408,36 @@ def run_warmstart(args, rank, world, local):
         print(json.dumps(line), flush=True)
 
 
+def gridding_roofline(n, na, lconv_adj, fwd_ms, adj_ms, pk=None):
+    """Roofline figures of one gridding forward and adjoint application: per
+    application na * pdim polar samples (both half-planes), each a
+    ceil(lconv)^2 window of complex64 taps (8 B and 8 flops a tap), plus the 2-D
+    FFT (5 pdim^2 log2(pdim^2) flops), against the L1 16-byte load rate and the
+    FP32 FMA rate measured now; and the HBM passes over the complex64 Fourier
+    grid (written once by the fill / gather, two read+write passes of the 2-D
+    FFT, read once by the gather / deapodisation) plus the na x pdim polar rows
+    written and read once, against the measured HBM copy rate.  The forward's
+    window width is the reference's fixed 2 * 7 / pi (gridrec_v4_forwproj.c);
+    the adjoint's is the plan's (param[6])."""
+    from iterative_tomographic_reconstruction_algorithms_b200.gridrec_lut import grid_size
+    pk = pk or onchip_peaks()
+    peaks_file = ROOT / "MEASURED_PEAKS.json"
+    hbm_peak = json.loads(peaks_file.read_text())["hbm_gbs"] if peaks_file.exists() else 6650.0
+    pdim = grid_size(n, 2.0)
+    roof = {}
+    for name, lconv, t_ms in (("forward", 2 * 7.0 / np.pi, fwd_ms), ("adjoint", lconv_adj, adj_ms)):
+        taps = float(na) * pdim * math.ceil(lconv) ** 2
+        flops = 8.0 * taps + 5.0 * pdim * pdim * math.log2(pdim * pdim)
+        gb = 8.0 * taps / (t_ms * 1e-3) / 1e9
+        tf = flops / (t_ms * 1e-3) / 1e12
+        hbm = 8.0 * (6.0 * pdim * pdim + 2.0 * na * pdim)
+        hb = hbm / (t_ms * 1e-3) / 1e9
+        roof[name] = {"ms": t_ms, "window": math.ceil(lconv), "gathered_gbs": gb, "frac_of_l1": gb / pk["l1_gbs"],
+                      "tflops": tf, "frac_of_fp32": tf / pk["fp32_tflops"],
+                      "hbm_bytes_passes": hbm, "hbm_gbs": hb, "frac_of_hbm": hb / hbm_peak}
+    return roof
+
+
 def admm_core(steps, warmup, dev, cpu_baseline=True):
     """ADMM-TV (admm.lasso_tv) with the gridding pair: 1024^2 phantom centred in
     1536 bins, 1500 angles on [0, 180), Kaiser-Bessel W = 6, oversampling 2
@@ -470,28 +500,7 @@ def admm_core(steps, warmup, dev, cpu_baseline=True):
     if cpu_baseline:
         cpu = admm_cpu_baseline(tp, b[0].cpu().numpy(), n, n2)
     upd = 12.0 * n * n * na  # 6 pairs of n^2 na updates per outer iteration
-    # gridding roofline: per application na * pdim polar samples (both half-planes), each a
-    # ceil(lconv)^2 window of complex64 taps (8 B and 8 flops a tap), plus the 2-D FFT
-    # (5 pdim^2 log2(pdim^2) flops); peaks: L1 16-byte loads and FP32 FMA, measured now
-    pk = onchip_peaks()
-    peaks_file = ROOT / "MEASURED_PEAKS.json"
-    hbm_peak = json.loads(peaks_file.read_text())["hbm_gbs"] if peaks_file.exists() else 6650.0
-    from iterative_tomographic_reconstruction_algorithms_b200.gridrec_lut import grid_size
-    pdim = grid_size(n, 2.0)
-    roof = {}
-    for name, lconv, t_ms in (("forward", 2 * 7.0 / np.pi, fwd_ms), ("adjoint", float(tp.param_nofilt[6]), adj_ms)):
-        taps = float(na) * pdim * math.ceil(lconv) ** 2
-        flops = 8.0 * taps + 5.0 * pdim * pdim * math.log2(pdim * pdim)
-        gb = 8.0 * taps / (t_ms * 1e-3) / 1e9
-        tf = flops / (t_ms * 1e-3) / 1e12
-        # HBM passes over the complex64 Fourier grid: written once (fill / gather), two
-        # read+write passes of the 2-D FFT, read once (gather / deapodise), plus the
-        # na x pdim polar rows written and read once
-        hbm = 8.0 * (6.0 * pdim * pdim + 2.0 * na * pdim)
-        hb = hbm / (t_ms * 1e-3) / 1e9
-        roof[name] = {"ms": t_ms, "window": math.ceil(lconv), "gathered_gbs": gb, "frac_of_l1": gb / pk["l1_gbs"],
-                      "tflops": tf, "frac_of_fp32": tf / pk["fp32_tflops"],
-                      "hbm_bytes_passes": hbm, "hbm_gbs": hb, "frac_of_hbm": hb / hbm_peak}
+    roof = gridding_roofline(n, na, float(tp.param_nofilt[6]), fwd_ms, adj_ms)
     out = {
         "metric": "ADMM-TV outer iterations per second (gridding pair, 5 inner CG iterations)",
         "value": 1e3 / ms, "unit": "iterations/s", "n_gpus": 1, "steps": steps, "warmup": warmup,
@@ -760,6 +769,9 @@ def run_kinds(args, rank, world, local):
                     r["gathered_gbs"] = gbs
                     r["frac_of_l1"] = gbs / pk["l1_gbs"]
                 res[name] = r
+            if kind == "grid":
+                res["roofline"] = gridding_roofline(n, na, float(tp.param_nofilt[6]), res["forward"]["ms"],
+                                                    res["adjoint"]["ms"], pk)
             out[kind] = res
             del tp
             torch.cuda.empty_cache()
