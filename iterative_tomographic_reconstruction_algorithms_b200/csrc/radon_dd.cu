@@ -26,14 +26,17 @@
 //            large).  The prefix sums take pixel widths as 1; the
 //            reference's are P_j+1 - P_j in float, which is 1 exactly except
 //            for pixels straddling a binade of P (|P| = 2^e), whose width
-//            differs by a rounding of q: those are added per line
-//            (dd_fwd_corr_kernel).  Angles whose coordinates reach 2^22 walk
-//            the pieces instead (dd_fwd_exact).
+//            differs by a rounding of q: those are added per line, and the
+//            dropped last piece of every line is subtracted, by a kernel of
+//            their own (dd_fwd_corr_kernel) into a float row per angle that
+//            the forward adds where it stores.  Angles whose coordinates
+//            reach 2^22 walk the pieces instead (dd_fwd_exact).
 //   adjoint  a pixel is at most one detector wide (r >= 1), so it overlaps the
 //            detector holding its left boundary and possibly the next: two
 //            float gaps, as the reference forms them, from one 8-byte table
 //            entry {S_a, S_a+1} per angle and the boundary D_a+1 recomputed.
-// The dropped last piece is subtracted where it falls (dd_dropped_piece).
+// The dropped last piece is subtracted where it falls (dd_dropped_piece):
+// forward in dd_fwd_corr_kernel, adjoint in the pixel loop.
 //
 // Work is described by a table of instances (one per slice, or per geometry
 // of an uneven batch) and consumed by persistent kernels: each warp takes the
@@ -362,13 +365,13 @@ __global__ void __launch_bounds__(kScanThreads) dd_sino_expand_kernel(const DdIn
 // ---------------------------------------------------------------------------
 // Forward: a warp item is 127 detectors of one angle; lane l holds the lower
 // boundaries of detectors B0 + 32 j + l (j = 0..3), and T_j = sum over lines of
-// F(boundary).  Lines whose dropped piece may belong to one of the item's
-// detectors form one contiguous band, where the piece is also subtracted.
+// F(boundary).  The dropped pieces and the binade corrections come from
+// dd_fwd_corr_kernel's row; keeping them out of this loop leaves it 64
+// registers (with them inline: 76, and 24 instead of 32 warps per SM).
 // ---------------------------------------------------------------------------
-template <bool BAND>
 __device__ __forceinline__ void dd_fwd_lines(int ia, int ib, const double2 *__restrict__ SL, int ws, float k,
-                                             float r, int n, int nh, int B0, int lane, const float (&Dlo)[4],
-                                             const float (&lo_nh)[4], double (&T)[4], double (&C)[4]) {
+                                             int n, int nh, const float (&Dlo)[4], const float (&lo_nh)[4],
+                                             double (&T)[4]) {
   float y = (float)(ia - nh) + 0.5f;
   const double2 *sl = SL + (size_t)ia * ws;
   const float nlim = (float)n + 0.25f, cmn = kMagic + (float)nh;
@@ -387,19 +390,6 @@ __device__ __forceinline__ void dd_fwd_lines(int ia, int ib, const double2 *__re
       const float Pk = __fsub_rn(__fsub_rn(f, cmn), q);
       const double2 e = __ldg(sl + kk);
       T[j] = fma((double)__fsub_rn(Dlo[j], Pk), e.y, T[j] + e.x);
-    }
-    if (BAND) {
-      DdDrop d;
-      if (dd_dropped_piece(q, r, n, nh, d)) {
-        const int rel = d.det - B0;
-        if (rel >= 0 && rel < kGrpDet && (rel & 31) == lane) {
-          const double amt = (double)d.gap * __ldg(&sl[d.pix].y);
-          const int jj = rel >> 5;
-#pragma unroll
-          for (int j = 0; j < 4; ++j)
-            if (j == jj) C[j] += amt;
-        }
-      }
     }
     y = __fadd_rn(y, 1.0f);
     sl += ws;
@@ -537,23 +527,27 @@ __device__ __forceinline__ void dd_fwd_exact(const double2 *__restrict__ SL, int
   }
 }
 
-// The binade corrections of every angle into the float rows X[v][m] that the
-// forward adds where it stores: one block per angle of every instance, its
-// warps taking the crossings in turn (dd_fwd_crossing); the crossings' sums
-// are then added into the row in crossing order through shared memory, so the
-// result is deterministic.  A launch of its own, so that the forward's
-// register budget is that of its main loop.
+// The binade corrections and the dropped pieces of every angle into the float
+// rows X[v][m] that the forward adds where it stores: one block per angle of
+// every instance, its warps taking the crossings in turn (dd_fwd_crossing);
+// the crossings' sums are added into the row in crossing order through shared
+// memory, then each line's dropped piece in line order, so the result is
+// deterministic.  A launch of its own, so that the forward's register budget
+// is that of its main loop.
 __device__ __forceinline__ bool dd_wide(float k, int nh) {
   return fabsf(k) * (float)(nh + 1) + (float)(nh + 2) >= 4194304.0f;
 }
 
 constexpr int kCorrWarps = 8, kCorrRow = 4096;  // rows longer than kCorrRow are added in global memory
+constexpr int kDropChunk = 1024;                 // lines whose dropped pieces are staged at a time
 
 __global__ void __launch_bounds__(32 * kCorrWarps) dd_fwd_corr_kernel(const DdInst *__restrict__ inst, int ninst,
                                                                       double2 *__restrict__ work) {
   __shared__ double sums[kNumCrossings][4];
   __shared__ int smc[kNumCrossings];
   __shared__ float row[kCorrRow];
+  __shared__ int ddet[kDropChunk];
+  __shared__ double damt[kDropChunk];
   const long long b = blockIdx.x;
   const DdInst &I = inst[find_inst(inst, ninst, b, &DdInst::s0)];
   const int v = (int)(b - I.s0), n = I.n, nh = I.nh, ws = n + 2;
@@ -578,14 +572,51 @@ __global__ void __launch_bounds__(32 * kCorrWarps) dd_fwd_corr_kernel(const DdIn
     else X[m] = 0.0f;
   }
   __syncthreads();
+  float *R = in_smem ? row : X;
   if (threadIdx.x == 0) {
-    float *R = in_smem ? row : X;
     for (int c = 0; c < kNumCrossings; ++c) {
       if (smc[c] == INT_MIN) continue;
       for (int t = 0; t < 4; ++t) {
         const int m = smc[c] - 1 + t;
         if (m >= 0 && m < n) R[m] += (float)sums[c][t];
       }
+    }
+  }
+  // The piece of every line the reference never credits (dd_dropped_piece),
+  // subtracted from its detector, line after line by one thread.
+  if (lines) {
+    for (int i0 = 0; i0 < n; i0 += kDropChunk) {
+      __syncthreads();
+      for (int t = threadIdx.x; t < kDropChunk && i0 + t < n; t += blockDim.x) {
+        const int i = i0 + t;
+        const float q = __fmul_rn(__fadd_rn((float)(i - nh), 0.5f), g.k);
+        DdDrop d;
+        int det = -1;
+        double amt = 0.0;
+        if (dd_dropped_piece(q, g.r, n, nh, d)) {
+          det = d.det;
+          amt = (double)d.gap * __ldg(&SL[(size_t)i * ws + d.pix].y);
+        }
+        ddet[t] = det;
+        damt[t] = amt;
+      }
+      __syncthreads();
+      // warp 0, 32 lines at a time: the lanes with the same detector form a
+      // group whose lowest lane subtracts the group's pieces summed in line
+      // order; different groups touch different detectors, and the batches
+      // go in line order
+      if (warp == 0)
+        for (int t0 = 0; t0 < kDropChunk && i0 + t0 < n; t0 += 32) {
+          const int t = t0 + lane;
+          const int det = i0 + t < n ? ddet[t] : -1;
+          const unsigned grp = __match_any_sync(0xffffffffu, det);
+          if (det >= 0 && lane == __ffs(grp) - 1) {
+            double sum = 0.0;
+            for (unsigned mk = grp; mk; mk &= mk - 1) sum += damt[t0 + __ffs(mk) - 1];
+            R[det] = __double2float_rn((double)R[det] - sum);
+          }
+          __syncwarp();
+        }
     }
   }
   __syncthreads();
@@ -621,16 +652,8 @@ __device__ __forceinline__ void dd_fwd_item(const DdInst &I, int v, int grp, int
     const int mEnd = min(B0 + kGrpDet, n);
     const double DA = (double)det_bound(B0, nh, r), DB = (double)det_bound(mEnd, nh, r);
     const double kd = (double)k, PN = (double)(n - nh);
-    int i0, i1, j0, j1;
+    int i0, i1;
     dd_line_range(-(double)nh - DB, PN - DA, kd, n, nh, i0, i1);
-    const double margin = 2.0 + 1e-6 * (fabs(DA) + fabs(DB) + (double)n * (1.0 + fabs(kd)));
-    dd_line_range(PN - (mEnd == n ? 1e30 : DB + margin), PN - (DA - margin), kd, n, nh, j0, j1);
-    j0 = max(j0, i0);
-    j1 = min(j1, i1);
-    if (j0 > j1) {
-      j0 = i1 + 1;
-      j1 = i1;
-    }
     if (dd_wide(k, nh)) {
       // |P| reaches 2^22: pieces walked exactly (rare near-axis angles)
       double T[4] = {0.0, 0.0, 0.0, 0.0};
@@ -638,10 +661,8 @@ __device__ __forceinline__ void dd_fwd_item(const DdInst &I, int v, int grp, int
 #pragma unroll
       for (int j = 0; j < 4; ++j) acc[j] = (float)T[j];
     } else {
-      double T[4] = {0.0, 0.0, 0.0, 0.0}, C[4] = {0.0, 0.0, 0.0, 0.0};
-      dd_fwd_lines<false>(i0, j0, SL, ws, k, r, n, nh, B0, lane, Dlo, lo_nh, T, C);
-      dd_fwd_lines<true>(j0, j1 + 1, SL, ws, k, r, n, nh, B0, lane, Dlo, lo_nh, T, C);
-      dd_fwd_lines<false>(j1 + 1, i1 + 1, SL, ws, k, r, n, nh, B0, lane, Dlo, lo_nh, T, C);
+      double T[4] = {0.0, 0.0, 0.0, 0.0};
+      dd_fwd_lines(i0, i1 + 1, SL, ws, k, n, nh, Dlo, lo_nh, T);
       // the upper boundary of detector B0 + 32 j + l is lane l+1's j-th, or lane 0's (j+1)-th
 #pragma unroll
       for (int j = 0; j < 4; ++j) {
@@ -652,7 +673,7 @@ __device__ __forceinline__ void dd_fwd_item(const DdInst &I, int v, int grp, int
         const float x = (32 * j + lane < kGrpDet && m < n)
                             ? __ldg(reinterpret_cast<const float *>(work + I.xs) + (size_t)v * n + m)
                             : 0.0f;
-        acc[j] = (float)(((up - T[j]) - C[j]) + (double)x);
+        acc[j] = (float)((up - T[j]) + (double)x);
       }
     }
   }
