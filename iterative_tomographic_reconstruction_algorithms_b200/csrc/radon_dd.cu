@@ -425,7 +425,7 @@ __device__ __forceinline__ int dd_fwd_kk(float lo_nh, float q, float nlim) {
 // butterfly, so deterministic).
 constexpr int kNumCrossings = 46;  // e = 0 .. 22, both signs
 
-__device__ __forceinline__ bool dd_fwd_crossing(const double2 *__restrict__ SL, int ws, float k, float r, int n,
+__device__ __forceinline__ bool dd_fwd_crossing(const float *__restrict__ V, int si, int sj, float k, float r, int n,
                                                 int nh, int c, int lane, int &mc, double (&a)[4]) {
   const int e = c >> 1, sg = c & 1;
   const float DA = det_bound(0, nh, r), DB = det_bound(n, nh, r);
@@ -475,7 +475,7 @@ __device__ __forceinline__ bool dd_fwd_crossing(const double2 *__restrict__ SL, 
       else if (dd_fwd_kk(__fadd_rn(det_bound(m + 1, nh, r), fnh), q, nlim) <= j) ++m;
       else break;
     }
-    const double amt = (double)delta * __ldg(&SL[(size_t)i * ws + j].y);
+    const double amt = (double)delta * (double)__ldg(V + (size_t)i * si + (size_t)j * sj);
 #pragma unroll
     for (int t = 0; t < 4; ++t)
       if (m == mc - 1 + t) a[t] += amt;
@@ -542,6 +542,7 @@ constexpr int kCorrWarps = 8, kCorrRow = 4096;  // rows longer than kCorrRow are
 constexpr int kDropChunk = 1024;                 // lines whose dropped pieces are staged at a time
 
 __global__ void __launch_bounds__(32 * kCorrWarps) dd_fwd_corr_kernel(const DdInst *__restrict__ inst, int ninst,
+                                                                      const float *__restrict__ img,
                                                                       double2 *__restrict__ work) {
   __shared__ double sums[kNumCrossings][4];
   __shared__ int smc[kNumCrossings];
@@ -550,16 +551,19 @@ __global__ void __launch_bounds__(32 * kCorrWarps) dd_fwd_corr_kernel(const DdIn
   __shared__ double damt[kDropChunk];
   const long long b = blockIdx.x;
   const DdInst &I = inst[find_inst(inst, ninst, b, &DdInst::s0)];
-  const int v = (int)(b - I.s0), n = I.n, nh = I.nh, ws = n + 2;
+  const int v = (int)(b - I.s0), n = I.n, nh = I.nh;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   float *X = reinterpret_cast<float *>(work + I.xs) + (size_t)v * n;
   const DdAngle g = I.ang[v];
   const bool lines = (g.mode == DD_ROWS || g.mode == DD_COLS) && !dd_wide(g.k, nh);
-  const double2 *SLr = work + I.sl + 1, *SL = g.mode == DD_ROWS ? SLr : SLr + (size_t)n * ws;
+  // pixel j of line i (an image row, or a column) read from the image itself:
+  // 17 MB that stay in L2, where the prefix tables' values (134 MB) would not
+  const float *V = img + I.img;
+  const int si = g.mode == DD_ROWS ? n : 1, sj = g.mode == DD_ROWS ? 1 : n;
   for (int c = warp; c < kNumCrossings; c += kCorrWarps) {
     int mc = 0;
     double a[4] = {0.0, 0.0, 0.0, 0.0};
-    const bool used = lines && dd_fwd_crossing(SL, ws, g.k, g.r, n, nh, c, lane, mc, a);
+    const bool used = lines && dd_fwd_crossing(V, si, sj, g.k, g.r, n, nh, c, lane, mc, a);
     if (lane == 0) {
       smc[c] = used ? mc : INT_MIN;
 #pragma unroll
@@ -595,7 +599,7 @@ __global__ void __launch_bounds__(32 * kCorrWarps) dd_fwd_corr_kernel(const DdIn
         double amt = 0.0;
         if (dd_dropped_piece(q, g.r, n, nh, d)) {
           det = d.det;
-          amt = (double)d.gap * __ldg(&SL[(size_t)i * ws + d.pix].y);
+          amt = (double)d.gap * (double)__ldg(V + (size_t)i * si + (size_t)d.pix * sj);
         }
         ddet[t] = det;
         damt[t] = amt;
@@ -1313,7 +1317,7 @@ int dd_forward(Plan &p, const float *d_img, float *d_sino, cudaStream_t s, const
   const int ni = (int)S.inst.size();
   dd_row_prefix_kernel<<<(unsigned)S.row_blocks, kScanThreads, 0, s>>>(S.d_inst, ni, d_img, work);
   dd_col_prefix_kernel<<<(unsigned)S.col_blocks, 32 * kColWarps, 0, s>>>(S.d_inst, ni, d_img, work);
-  dd_fwd_corr_kernel<<<(unsigned)S.sino_blocks, 32 * kCorrWarps, 0, s>>>(S.d_inst, ni, work);
+  dd_fwd_corr_kernel<<<(unsigned)S.sino_blocks, 32 * kCorrWarps, 0, s>>>(S.d_inst, ni, d_img, work);
   TOMO_CUDA(cudaGetLastError());
   return dd_launch_fwd(S, S.wf, S.grid_f, work, d_sino, s, ep);
 }
