@@ -46,7 +46,7 @@ WORKLOAD = "distance-driven pair, 2048x2048 image, 1800 angles [0,180), 2048 bin
 TAU_DD = 2  # gathered operand values per update (distance-driven)
 # DRAM bytes per launch of the two main kernels at 2048^2 x 1800, from one ncu capture
 # (dram__bytes_read.sum + dram__bytes_write.sum)
-DRAM_BYTES_PER_LAUNCH = {"forward": 139.65e6 + 15.33e6, "adjoint": 37.99e6 + 0.0064e6}
+DRAM_BYTES_PER_LAUNCH = {"forward": 153.6e6 + 10.0e6, "adjoint": 38.0e6 + 0.0064e6}
 
 
 def parse():
