@@ -172,7 +172,7 @@ struct DdInst {
   long long img, sino;   // offsets (floats) of the image / sinogram in the packed arrays
   long long sl;          // offset (double2) of the row prefix lines; column lines follow
   long long as;          // offset (double2) of the sinogram prefix rows [na][w2]
-  long long xs;          // offset (double2) of the forward's width corrections, float [na][n]
+  long long xs;          // offset (double2) of the forward's corrections, float [na][n], or the adjoint's dropped-piece image [n][n]
   long long f0, a0;      // first forward / adjoint work item
   long long r0, c0, s0;  // first row-prefix / column-prefix / sinogram-prefix block
   const DdAngle *ang;    // [na] per-angle geometry, angle order
@@ -776,15 +776,12 @@ __device__ __forceinline__ void dd_adj_pass(const float4 *__restrict__ tab, int 
   float x[5];
 #pragma unroll
   for (int j = 0; j < 5; ++j) x[j] = (float)(k0 - nh + j);
-  const bool lastpix = k0 + 3 >= n - 1;
   const float cm = kMagic + (float)nh, cm1 = cm - 1.0f;
 #pragma unroll 1
   for (int u = 0; u < cnt; ++u) {
     const float4 e = __ldg(tab + u);
     const float r = e.x, k = e.y, z = e.z;
-    const float2 *row = AS + __float_as_int(e.w);
-    const float2 *rowm = row - kMagicBits;
-    const float Dn = det_bound(n, nh, r);
+    const float2 *rowm = AS + __float_as_int(e.w) - kMagicBits;
 #pragma unroll
     for (int li = 0; li < 4; ++li) {
       const float q = __fmul_rn(__fadd_rn(y0, (float)li), k);
@@ -793,16 +790,57 @@ __device__ __forceinline__ void dd_adj_pass(const float4 *__restrict__ tab, int 
       for (int j = 0; j < 5; ++j) P[j] = __fsub_rn(x[j], q);
 #pragma unroll
       for (int j = 0; j < 4; ++j) dd_adj_pixel(P[j], P[j + 1], z, r, cm, cm1, rowm, COLS ? acc[j][li] : acc[li][j]);
-      if (lastpix || (P[0] < Dn && Dn < P[4])) {
-        DdDrop d;
-        if (dd_dropped_piece(q, r, n, nh, d)) {
-          const float sd = __fmul_rn(d.gap, __ldg(&row[d.det].x));
-#pragma unroll
-          for (int j = 0; j < 4; ++j)  // unrolled: acc stays in registers
-            if (d.pix == k0 + j) (COLS ? acc[j][li] : acc[li][j]) -= sd;
-        }
+    }
+  }
+}
+
+// The adjoint's dropped pieces (the last piece of each line and angle that
+// the reference never credits, dd_dropped_piece), as an image C that the
+// adjoint adds where it stores: a warp per line (an image row for the angles
+// on rows, a column for those on columns), 32 angles at a time; the lanes
+// whose pieces fall on the same pixel form a group whose lowest lane
+// subtracts their sum, taken in angle order, from C.  The row launch zeroes
+// its lines first and runs before the column launch, so every pixel gets its
+// pieces in one fixed order.  Out of the adjoint's main loop, which then holds
+// 64 registers (with the pieces inline: 80, and 24 instead of 32 warps per SM).
+template <bool COLS>
+__global__ void __launch_bounds__(32) dd_adj_drop_kernel(const DdInst *__restrict__ inst, int ninst,
+                                                         double2 *__restrict__ work) {
+  __shared__ double samt[32];
+  const long long b = blockIdx.x;
+  const DdInst &I = inst[find_inst(inst, ninst, b, &DdInst::r0)];
+  const int l = (int)(b - I.r0), n = I.n, nh = I.nh, lane = threadIdx.x;
+  float *C = reinterpret_cast<float *>(work + I.xs);
+  const size_t si = COLS ? 1 : (size_t)n, sp = COLS ? (size_t)n : 1;  // pixel p of line l: C[l si + p sp]
+  if (!COLS)
+    for (int p = lane; p < n; p += 32) C[(size_t)l * n + p] = 0.0f;
+  __syncwarp();
+  const float4 *tab = I.tab + (COLS ? I.nR : 0);
+  const int cnt = COLS ? I.nC : I.nR;
+  const float2 *AS = (const float2 *)(work + I.as) + I.pads;
+  const float y = __fadd_rn((float)(l - nh), 0.5f);
+  for (int u0 = 0; u0 < cnt; u0 += 32) {
+    const int u = u0 + lane;
+    int pix = -1;
+    float amt = 0.0f;
+    if (u < cnt) {
+      const float4 e = __ldg(tab + u);
+      DdDrop d;
+      if (dd_dropped_piece(__fmul_rn(y, e.y), e.x, n, nh, d)) {
+        pix = d.pix;
+        amt = __fmul_rn(d.gap, __ldg(&(AS + __float_as_int(e.w))[d.det].x));
       }
     }
+    samt[lane] = (double)amt;
+    __syncwarp();
+    const unsigned grp = __match_any_sync(0xffffffffu, pix);
+    if (pix >= 0 && lane == __ffs(grp) - 1) {
+      double sum = 0.0;
+      for (unsigned mk = grp; mk; mk &= mk - 1) sum += samt[__ffs(mk) - 1];
+      float *c = C + (size_t)l * si + (size_t)pix * sp;
+      *c = __double2float_rn((double)*c - sum);
+    }
+    __syncwarp();
   }
 }
 
@@ -879,12 +917,15 @@ __global__ void __launch_bounds__(128 * TB) dd_adj_kernel(const DdInst *__restri
 #pragma unroll
           for (int j = 0; j < 4; ++j) acc[i][j] += __ldg(&row[e.x == DD_ROWSUM ? a0 + i : b0 + j].x);
       }
+      // the dropped pieces (dd_adj_drop_kernel)
+      const float *Cimg = reinterpret_cast<const float *>(work + I.xs);
 #pragma unroll
       for (int i = 0; i < 4; ++i)
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
           const int a = a0 + i, b = b0 + j;
           const bool live = inside && a < n && b < n;
+          if (live) acc[i][j] += __ldg(Cimg + (size_t)a * n + b);
           adj_store(ep, acc[i][j], live, (size_t)I.img + (size_t)(live ? a : 0) * n + (live ? b : 0), img);
         }
     }
@@ -1225,8 +1266,10 @@ int dd_build(Plan &p, const DdGeo *geo, int count) {
   for (int idx : order) work += 2 * (size_t)inst[idx].n * (inst[idx].n + 2);
   size_t sl_at = 0, as_at = work;
   for (int idx : order) work += (size_t)inst[idx].na * inst[idx].w2;
-  size_t xs_at = work;  // float rows, 4 to a double2
-  for (int idx : order) work += ((size_t)inst[idx].na * inst[idx].n + 3) / 4;
+  // float rows, 4 to a double2: the forward's corrections [na][n] or, in an
+  // adjoint, the dropped-piece image [n][n] (never both at once)
+  size_t xs_at = work;
+  for (int idx : order) work += ((size_t)std::max(inst[idx].na, inst[idx].n) * inst[idx].n + 3) / 4;
   for (int idx : order) {
     DdInst I = inst[idx];
     I.sl = (long long)sl_at;
@@ -1234,7 +1277,7 @@ int dd_build(Plan &p, const DdGeo *geo, int count) {
     I.as = (long long)as_at;
     as_at += (size_t)I.na * I.w2;
     I.xs = (long long)xs_at;
-    xs_at += ((size_t)I.na * I.n + 3) / 4;
+    xs_at += ((size_t)std::max(I.na, I.n) * I.n + 3) / 4;
     I.f0 = S->fwd_items;
     S->fwd_items += (long long)I.na * I.ngrp;
     I.a0 = S->adj_items;
@@ -1327,6 +1370,8 @@ int dd_adjoint(Plan &p, const float *d_sino, float *d_img, cudaStream_t s, const
   double2 *work = (double2 *)p.d_scratch;
   const int ni = (int)S.inst.size();
   dd_sino_expand_kernel<<<(unsigned)S.sino_blocks, kScanThreads, 0, s>>>(S.d_inst, ni, d_sino, work);
+  dd_adj_drop_kernel<false><<<(unsigned)S.row_blocks, 32, 0, s>>>(S.d_inst, ni, work);
+  dd_adj_drop_kernel<true><<<(unsigned)S.row_blocks, 32, 0, s>>>(S.d_inst, ni, work);
   TOMO_CUDA(cudaGetLastError());
   return dd_launch_adj(S, S.wa, S.grid_a, work, d_img, s, ep);
 }
