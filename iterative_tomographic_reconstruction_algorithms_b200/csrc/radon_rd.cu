@@ -16,8 +16,9 @@
 // slice) replaying its bin's five sub-rays:
 //   forward  gathers 0.2 l x[pixel] into the bin, in walk order;
 //   adjoint  scatters 0.2 l y[bin] into a 64-bit fixed-point image with
-//            integer atomics (order-independent sums, so deterministic, of
-//            credits rounded to the fixed-point unit), rounded to float once, through the solver epilogue, at the end.
+//            integer reductions (order-independent sums, so deterministic, of
+//            credits rounded to the fixed-point unit), rounded to float once,
+//            through the solver epilogue, at the end.
 //            Non-finite credits (inf or NaN in y, or 0 * inf) cannot be held
 //            as integers: they set per-pixel flags instead, and a flagged
 //            pixel becomes what the reference's float sum gives (+inf, -inf,
@@ -26,7 +27,10 @@
 // side across the ray.  For angles whose rays run along image columns
 // (|s| > |c|) that is down a column: those angles read a transposed copy of
 // the image (forward) and scatter into a transposed fixed-point image
-// (adjoint), so neighbouring lanes touch neighbouring words.
+// (adjoint), so neighbouring lanes touch neighbouring words.  Both copies are
+// framed (rows and columns -1 .. n+1, zero or ignored outside [1, n-1]^2), so
+// that the walks whose end points lie within nh + 1/4 of the centre -- all of
+// them but for rounding -- run without a range test (rd_walk_framed).
 // The walk's arithmetic is float only: the crossing parameters reproduce the
 // reference's double quotients exactly (rd_alpha_mf), with a double division
 // only for quotients within 2^-38 of a float rounding boundary.
