@@ -68,6 +68,11 @@ def parse():
     ap.add_argument("--train-pairs", type=int, default=2048, help="warmstart: training samples")
     ap.add_argument("--train-steps", type=int, default=2000, help="warmstart: training steps")
     ap.add_argument("--eval-slices", type=int, default=256, help="warmstart: held-out slices")
+    ap.add_argument("--compact-pairs", action="store_true",
+                    help="warmstart: keep training samples in bf16 without x_ref (for 20k samples)")
+    ap.add_argument("--save-net", default=None, help="warmstart: write the trained network's weights here")
+    ap.add_argument("--load-net", default=None,
+                    help="warmstart: evaluate the network with these weights instead of training one")
     ap.add_argument("--no-blocks", action="store_true",
                     help="pair workload: skip the C1-C5 blocks measured after the headline")
     ap.add_argument("--block-slices", type=int, default=512, help="C4 block: slices")
@@ -342,7 +347,8 @@ def oracle_residuals(xs, b, na, threads=None):
     return out
 
 
-def warmstart_core(train_pairs, train_steps, eval_slices, lam, dev, oracle_slices=2):
+def warmstart_core(train_pairs, train_steps, eval_slices, lam, dev, oracle_slices=2, compact=False,
+                   save_net=None, load_net=None):
     """Learned warm start at 512^2 (768 bins), 180 angles on [0, 180), Poisson I0 = 5e3:
     samples (2-iteration SIRT, filtered backprojection, 300-iteration SIRT, phantom)
     generated by the batched solver on seeds 10000 + i, a 4-level, 32-channel U-Net
@@ -355,17 +361,24 @@ def warmstart_core(train_pairs, train_steps, eval_slices, lam, dev, oracle_slice
     import torch
     from iterative_tomographic_reconstruction_algorithms_b200 import nn, warmstart as ws
     pb = ws.Problem()
-    t0 = time.perf_counter()
-    data = ws.make_pairs(pb, [10000 + i for i in range(train_pairs)])
-    torch.cuda.synchronize()
-    t_pairs = time.perf_counter() - t0
     net = nn.UNet(levels=4, base=32, seed=0).to(dev)
-    t0 = time.perf_counter()
-    hist = ws.train(net, pb, data, steps=train_steps, batch=4, lam=lam)
-    torch.cuda.synchronize()
-    t_train = time.perf_counter() - t0
-    del data
-    torch.cuda.empty_cache()
+    if load_net:  # weights of an earlier run of the same training (save_net)
+        net.load_state_dict(torch.load(load_net, map_location=dev))
+        t_pairs = t_train = None
+        hist = []
+    else:
+        t0 = time.perf_counter()
+        data = ws.make_pairs(pb, [10000 + i for i in range(train_pairs)], compact=compact)
+        torch.cuda.synchronize()
+        t_pairs = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        hist = ws.train(net, pb, data, steps=train_steps, batch=4, lam=lam)
+        torch.cuda.synchronize()
+        t_train = time.perf_counter() - t0
+        del data
+        torch.cuda.empty_cache()
+        if save_net:
+            torch.save(net.state_dict(), save_net)
     r = ws.time_to_residual(net, pb, [100000 + i for i in range(eval_slices)])
     k = min(oracle_slices, eval_slices)
     bh = r["b"][:k].cpu().numpy()
@@ -381,7 +394,9 @@ def warmstart_core(train_pairs, train_steps, eval_slices, lam, dev, oracle_slice
            "config": {"workload": "512^2 phantom in 768 bins, 180 angles, Poisson I0=5e3, dd pair, SIRT from 0; "
                                   "U-Net 4 levels x 32 channels, BF16 weights/activations, FP32 accumulation",
                       "train_pairs": train_pairs, "train_steps": train_steps, "lam": lam,
-                      "eval_slices": eval_slices},
+                      "eval_slices": eval_slices,
+                      "stored_samples": "bf16 x2/fbp/x_true, no x_ref" if compact else "f32",
+                      "network": f"loaded from {load_net}" if load_net else "trained in this run"},
            "plain_ms": r["plain_ms"], "warm_ms": r["warm_ms"], "warm_iters": r["warm_iters"],
            "plain_iters": r["plain_iters"], "residual_plain": r["residual_plain"],
            "residual_warm": r["residual_warm"], "image_rel_err_plain": r["err_plain"],
@@ -399,7 +414,8 @@ def run_warmstart(args, rank, world, local):
     import torch
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
-    r = warmstart_core(args.train_pairs, args.train_steps, args.eval_slices, args.lam, dev)
+    r = warmstart_core(args.train_pairs, args.train_steps, args.eval_slices, args.lam, dev,
+                       compact=args.compact_pairs, save_net=args.save_net, load_net=args.load_net)
     if rank == 0:
         line = {"metric": "learned warm start: GPU time to reach plain SIRT's 300-iteration data residual, warm / plain",
                 "n_gpus": 1, "steps": 1, "warmup": 1, "ms_per_step": r["warm_ms"], "scaling": "weak",

@@ -77,22 +77,31 @@ def fbp(tp, b):
     return tp.At(f) * (math.pi / na)
 
 
-def make_pairs(pb: Problem, seeds, chunk: int = 64, device="cuda"):
+def make_pairs(pb: Problem, seeds, chunk: int = 64, device="cuda", compact: bool = False):
     """Training samples on the GPU, ``chunk`` slices per batched solve: a dict of
-    x2, fbp, x_ref, x_true, b and r_ref (the reference's data residual per slice)."""
-    out = {k: [] for k in ("x2", "fbp", "x_ref", "x_true", "b", "r_ref")}
+    x2, fbp, x_ref, x_true, b and r_ref (the reference's data residual per slice).
+
+    ``compact``: for large sample counts (20k samples at 768^2 hold ~200 GB in
+    float32) x2, fbp and x_true are kept in bfloat16 (the network's operand
+    type; ``train`` widens them to float32 per batch) and x_ref is not kept
+    (training uses only r_ref): ~4 MB a sample."""
+    keys = ("x2", "fbp", "x_true", "b", "r_ref") if compact else ("x2", "fbp", "x_ref", "x_true", "b", "r_ref")
+    low = (lambda t: t.to(torch.bfloat16)) if compact else (lambda t: t)
+    out = {k: [] for k in keys}
     for i in range(0, len(seeds), chunk):
         x_true, b, tp = make_batch(pb, seeds[i:i + chunk], device)
         zero = torch.zeros((b.shape[0], pb.n_op, pb.n_op), device=device)
         solver = Solver(tp, "sirt", b)
         x2, _ = solver.run(zero, pb.start_iters)
         xr, _ = solver.run(x2, pb.ref_iters - pb.start_iters)
-        out["x2"].append(x2)
-        out["fbp"].append(fbp(tp, b))
-        out["x_ref"].append(xr)
-        out["x_true"].append(x_true)
+        out["x2"].append(low(x2))
+        out["fbp"].append(low(fbp(tp, b)))
+        if not compact:
+            out["x_ref"].append(xr)
+        out["x_true"].append(low(x_true))
         out["b"].append(b)
         out["r_ref"].append(((tp.A(xr) - b) ** 2).sum(dim=(1, 2)))
+        del solver, xr
     return {k: torch.cat(v) for k, v in out.items()}
 
 
@@ -116,7 +125,7 @@ def train(net, pb: Problem, data, steps: int = 1000, batch: int = 4, lr: float =
     for step in range(1, steps + 1):
         opt.lr = lr * 0.5 * (1.0 + math.cos(math.pi * (step - 1) / steps))
         idx = torch.randint(0, n, (batch,), generator=g).to(data["x2"].device)
-        xi, fi, ti = data["x2"][idx], data["fbp"][idx], data["x_true"][idx]
+        xi, fi, ti = data["x2"][idx].float(), data["fbp"][idx].float(), data["x_true"][idx].float()
         bi, rr = data["b"][idx].contiguous(), data["r_ref"][idx]
         if W is None:
             W = sirt_weights(op, xi)
@@ -135,9 +144,14 @@ def train(net, pb: Problem, data, steps: int = 1000, batch: int = 4, lr: float =
 
 
 @torch.no_grad()
-def warm_start(net, pb: Problem, x2, tp, b):
-    """f(x2, fbp(b)), or x2 for the slices where f has the larger data residual (fallback)."""
-    xw = apply_net(net, pb, x2, fbp(tp, b))
+def warm_start(net, pb: Problem, x2, tp, b, chunk: int = 64):
+    """f(x2, fbp(b)), or x2 for the slices where f has the larger data residual
+    (fallback).  The network runs on ``chunk`` slices at a time (its activations
+    at 768^2 take ~50 MB a slice)."""
+    fb = fbp(tp, b)
+    xw = torch.empty_like(x2)
+    for i in range(0, x2.shape[0], chunk):
+        xw[i:i + chunk] = apply_net(net, pb, x2[i:i + chunk], fb[i:i + chunk])
     rw = ((tp.A(xw) - b) ** 2).sum(dim=(1, 2))
     r2 = ((tp.A(x2) - b) ** 2).sum(dim=(1, 2))
     keep = (rw <= r2)[:, None, None]
