@@ -390,6 +390,20 @@ static int stage_out(Plan &p, const void *src, void *dst, size_t bytes) {
   return TOMO_OK;
 }
 
+// Touches every page of the output array (one byte per 4 KiB, overwritten by
+// the result later) on the pool while the projector runs: a freshly allocated
+// array would otherwise take its first-touch page faults inside the copies
+// out, after the device has finished.
+static void prefault_out(void *dst, size_t bytes) {
+  constexpr size_t kPage = 4096;
+  const size_t nch = (bytes + kStageChunk - 1) / kStageChunk;
+  volatile char *b = (volatile char *)dst;
+  StagePool::get().run((int)nch, [&](int c) {
+    const size_t off = (size_t)c * kStageChunk, end = std::min(bytes, off + kStageChunk);
+    for (size_t o = off; o < end; o += kPage) b[o] = 0;
+  });
+}
+
 static int host_call(tomo_plan *plan, const float *h_in, float *h_out, bool forward) {
   if (!plan || !h_in || !h_out) return fail(TOMO_EINVAL, "host call: NULL argument");
   Plan &p = plan->p;
@@ -403,6 +417,7 @@ static int host_call(tomo_plan *plan, const float *h_in, float *h_out, bool forw
   rc = forward ? tomo_forward(plan, p.d_in, p.d_out, p.host_stream)
                : tomo_adjoint(plan, p.d_in, p.d_out, p.host_stream);
   if (rc) return rc;
+  prefault_out(h_out, out_b);
   if (p.h_stage) {
     rc = stage_out(p, p.d_out, h_out, out_b);
     if (rc) return rc;
