@@ -960,7 +960,9 @@ def main():
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": WORKLOAD, "slices_per_rank_per_step": 1,
                        "l2": "flushed between steps (256 MiB write)", "parallelism": f"slices x{world}"},
-            "gpu_launches": 5 * args.steps,
+            # per step, forward: row and column prefix sums, corrections, main kernel;
+            # adjoint: sinogram expansion, dropped pieces (rows, columns), main kernel
+            "gpu_launches": 8 * args.steps,
             "kernel_ms": {"dd_forward (line prefix sums + persistent forward)": fwd_ms,
                           "dd_adjoint (sinogram prefix sums + persistent adjoint)": adj_ms},
             "tuning": _lib.plan_tuning(tp.plan(1, dev.index if hasattr(dev, "index") else 0)),
