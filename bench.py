@@ -86,27 +86,35 @@ def parse():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """nvidia-smi clocks and throttle reasons sampled during the timed region:
+    every 25 ms, with nvidia-smi's own timestamps, keeping the samples taken
+    between entering and leaving the ``with`` block (the sampler is started
+    and given half a second to come up before the block's region begins)."""
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    Q = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    PERIOD_MS = 25
 
     def __init__(self, index: int):
         self.index = index
         self.proc = None
+        self.t_begin = self.t_end = None
 
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", str(self.PERIOD_MS)],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            time.sleep(0.5)
         except OSError:
             self.proc = None
+        self.t_begin = time.time()
         return self
 
     def __exit__(self, *a):
+        self.t_end = time.time()
         self.lines = []
         if self.proc is not None:
             self.proc.terminate()
@@ -117,17 +125,28 @@ class ClockSampler:
                 out, _ = self.proc.communicate()
             self.lines = [l for l in out.splitlines() if l.strip()]
 
+    def _in_region(self, stamp: str) -> bool:
+        import datetime
+        try:
+            t = datetime.datetime.strptime(stamp.strip(), "%Y/%m/%d %H:%M:%S.%f").timestamp()
+        except ValueError:
+            return False
+        margin = self.PERIOD_MS * 1e-3
+        return self.t_begin - margin <= t <= self.t_end + margin
+
     def summary(self):
         sm, mx, reasons = [], 0.0, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for l in getattr(self, "lines", []):
             f = [x.strip() for x in l.split(",")]
-            try:
-                sm.append(float(f[1]))
-                mx = max(mx, float(f[2]))
-            except (ValueError, IndexError):
+            if len(f) < 10 or not self._in_region(f[0]):
                 continue
-            for nm, val in zip(names, f[5:9]):
+            try:
+                sm.append(float(f[2]))
+                mx = max(mx, float(f[3]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, f[6:10]):
                 if val.lower().startswith("active"):
                     reasons.add(nm)
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx or None,
