@@ -1,4 +1,6 @@
-"""Slices across GPUs: one process per GPU, independent slices, no data-path collective.
+"""Work across GPUs, one process per GPU.
+
+Slices: independent slices, no data-path collective.
 
 The reference's only parallelism is a process pool over independent slices
 (algorithms/art.py:289, sir.py:260).  Here each rank takes a share of the
@@ -11,6 +13,11 @@ results to rank 0 at the end (host side, any torch.distributed backend).
   mine = parts[rank]                          # indices into the slice list
   ...reconstruct slices `mine`...
   full = gather_to_root(results, mine, n)     # rank 0: list of n results
+
+One huge slice: its angles (AngleShardedProjector).  Each rank holds a plan for
+a contiguous range of the angles; the forward needs no communication (its rows
+are a contiguous block of the full sinogram), and the adjoint's partial images
+are summed by one all-reduce of 4 n^2 bytes.
 """
 from __future__ import annotations
 
@@ -85,3 +92,94 @@ def max_over_ranks(value: float, group=None) -> float:
         t = t.cuda()
     dist.all_reduce(t, op=dist.ReduceOp.MAX, group=group)
     return float(t.item())
+
+
+# Radon kinds whose plans write angle v's projection to row na - 1 - v
+# (radon_dd.c:79,181,273; radon_ss.c:111); the others write row v.
+_REVERSED_ROWS = {2, 3}  # TOMO_KIND_DD, TOMO_KIND_SS
+
+
+def angle_shards(na: int, world: int):
+    """Contiguous angle ranges [start, stop), one per rank, as equal as the
+    count allows (every angle of a Radon projector costs the same)."""
+    if world < 1:
+        raise ValueError("world must be >= 1")
+    base, extra = divmod(na, world)
+    out, start = [], 0
+    for r in range(world):
+        stop = start + base + (1 if r < extra else 0)
+        out.append((start, stop))
+        start = stop
+    return out
+
+
+class AngleShardedProjector:
+    """One slice whose angles are split across the ranks of ``group``.
+
+    ``make_plan(sub_angles)`` builds this rank's plan for its contiguous share
+    of ``angles`` (an object with ``forward(x)`` and ``adjoint(y)`` on CUDA
+    float32 tensors, e.g. ``_lib.Plan(kind, n, sub_angles)``); ``kind`` is the
+    Radon kind (TOMO_KIND_PD / RD / DD / SS), which fixes where the plan puts
+    each angle's row.
+
+    ``forward(x)``: this rank's rows, which are the full sinogram's rows
+    ``rows`` (a contiguous block); ``gather=True`` returns the full sinogram on
+    every rank instead (one all-gather).  ``adjoint(y_rows)``: this rank's
+    rows in, the full adjoint on every rank out: the partial images are summed
+    by an all-reduce (NCCL's order, fixed for a given set of ranks, so
+    deterministic; the sum is taken in another order than on one GPU, so equal
+    to it up to rounding).  With no process group (or one rank) both are the
+    plan's own results.
+    """
+
+    def __init__(self, make_plan, kind: int, angles, group=None):
+        import torch.distributed as dist
+        self.group = group
+        self.dist = dist.is_available() and dist.is_initialized()
+        self.rank = dist.get_rank(group) if self.dist else 0
+        self.world = dist.get_world_size(group) if self.dist else 1
+        angles = list(angles)
+        self.na = len(angles)
+        self.shards = angle_shards(self.na, self.world)
+        start, stop = self.shards[self.rank]
+        self.local = stop - start
+        self.plan = make_plan(angles[start:stop]) if self.local > 0 else None
+        # full-sinogram rows of this rank's rows: angle v's row is v, or na - 1 - v
+        first = (self.na - stop) if int(kind) in _REVERSED_ROWS else start
+        self.rows = slice(first, first + self.local)
+        self.row_starts = [((self.na - b) if int(kind) in _REVERSED_ROWS else a) for a, b in self.shards]
+
+    def forward(self, x, gather: bool = False):
+        import torch
+        n = x.shape[-1]
+        mine = self.plan.forward(x) if self.plan is not None else torch.zeros(
+            (0, n), dtype=torch.float32, device=x.device)
+        mine = mine.reshape(self.local, n)
+        if not gather:
+            return mine
+        full = torch.empty((self.na, n), dtype=torch.float32, device=x.device)
+        if self.world == 1:
+            full[self.rows] = mine
+            return full
+        import torch.distributed as dist
+        # all-gather takes equal sizes: every block padded to the largest share
+        m = max(b - a for a, b in self.shards)
+        padded = torch.zeros((m, n), dtype=torch.float32, device=x.device)
+        padded[:self.local] = mine
+        parts = [torch.empty((m, n), dtype=torch.float32, device=x.device) for _ in self.shards]
+        dist.all_gather(parts, padded, group=self.group)
+        for (a, b), r0, part in zip(self.shards, self.row_starts, parts):
+            full[r0:r0 + (b - a)] = part[:b - a]
+        return full
+
+    def adjoint(self, y_rows):
+        import torch
+        n = y_rows.shape[-1]
+        if self.plan is not None:
+            img = self.plan.adjoint(y_rows.reshape(self.local, n).contiguous()).reshape(n, n)
+        else:
+            img = torch.zeros((n, n), dtype=torch.float32, device=y_rows.device)
+        if self.world > 1:
+            import torch.distributed as dist
+            dist.all_reduce(img, op=dist.ReduceOp.SUM, group=self.group)
+        return img
