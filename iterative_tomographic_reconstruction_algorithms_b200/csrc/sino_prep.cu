@@ -17,7 +17,10 @@
 //     interpolated with the Keys cubic-convolution kernel (a = -1/2; R. Keys,
 //     IEEE Trans. ASSP 29(6), 1981), which reproduces quadratics exactly.
 //     The two interpolants agree to about 1e-3 of the signal on smooth data;
-//     this is not a bit-exact restatement.
+//     this is not a bit-exact restatement, nor can one be: the reference's
+//     own result moves by as much when only the order of its input points
+//     changes (Qhull's triangulation of the regular grid picks one of two
+//     equally valid diagonals per cell, following that order).
 // One thread per output element, coalesced along the detector axis.
 #include <cmath>
 
