@@ -372,11 +372,18 @@ __device__ __forceinline__ FixedScale rd_adj_scale(const unsigned *smax, int na)
 // frame and row / column 0 collect credits the reference does not make, which
 // the finalize ignores.  The row / column-sum angles add their one credit per
 // pixel to per-column (cols) and per-row (rows) sums instead.
+// kSplit: one thread per sub-ray (thread t walks sub-ray t % 5 + 1 of bin
+// t / 5) instead of one per bin walking all five, for grids too small to fill
+// the GPU; the sums are order-independent, so both give the same bits.  The
+// bin's first thread alone makes its row / column sum and non-finite flags.
+template <bool kSplit>
 __global__ void __launch_bounds__(128) rd_scatter_kernel(
     const float *__restrict__ sino, unsigned long long *__restrict__ accf, unsigned long long *__restrict__ accT,
     unsigned long long *__restrict__ lines, unsigned *__restrict__ flags, const RdAngle *__restrict__ tab,
     const float *__restrict__ toff, int n, int nh, int na, const unsigned *__restrict__ smax) {
-  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int b = kSplit ? t / 5 : t;
+  const int r0 = kSplit ? t - 5 * b + 1 : 1, r1 = kSplit ? r0 : 5;
   const int v = blockIdx.y;
   const size_t z = blockIdx.z;
   if (b >= n) return;
@@ -384,9 +391,10 @@ __global__ void __launch_bounds__(128) rd_scatter_kernel(
   if (y == 0.0f) return;
   const RdAngle g = tab[v];
   if (!(fabsf(y) <= 3.4028235e38f)) {  // inf or NaN
-    rd_scatter_nonfinite(y, tab + v, b, n, nh, toff, flags + z * (((size_t)n * n + 3) / 4));
+    if (r0 == 1) rd_scatter_nonfinite(y, tab + v, b, n, nh, toff, flags + z * (((size_t)n * n + 3) / 4));
     return;
   }
+  if (g.mode != 0 && r0 != 1) return;
   const FixedScale fs = rd_adj_scale(smax + z, na);
   const int m = n + 3;
   unsigned long long *cols = lines + z * 2 * (size_t)n, *rows = cols + n;
@@ -403,7 +411,7 @@ __global__ void __launch_bounds__(128) rd_scatter_kernel(
   unsigned long long *P = (tr ? accT : accf) + z * (size_t)m * m;
   const int sA = tr ? 1 : m, sB = tr ? m : 1;
   RdScatter add{P, __fmul_rn(__fmul_rn(y, fs.s1), fs.s2)};
-  for (int r = 1; r <= 5; ++r) {
+  for (int r = r0; r <= r1; ++r) {
     const RdGeom s = rd_geom_of(tab, v, toff, 6 * b + r, n, nh);
     const float rx = __frcp_rn(s.ex), ry = __frcp_rn(s.ey);
     if (rd_walk_framed(s, nh, rx, ry))
@@ -533,9 +541,16 @@ int rd_adjoint(Plan &p, const float *d_sino, float *d_img, cudaStream_t s, const
     TOMO_CUDA(cudaMemsetAsync(accT, 0, sizeof(unsigned long long) * zc * per_fr, s));
     TOMO_CUDA(cudaMemsetAsync(lines, 0, sizeof(unsigned long long) * zc * 2 * (size_t)n, s));
     TOMO_CUDA(cudaMemsetAsync(flags, 0, sizeof(unsigned) * zc * fw, s));
-    rd_scatter_kernel<<<dim3((n + 127) / 128, na, zc), 128, 0, s>>>(
-        d_sino + (size_t)z0 * per_sino, accf, accT, lines, flags, (const RdAngle *)p.d_angles,
-        (const float *)p.d_aux, n, p.nh, na, smax + z0);
+    // one thread per bin when that fills the GPU (148 SMs x 1024 threads at
+    // the kernel's 64 registers), else one per sub-ray
+    if ((size_t)n * na * zc >= (size_t)148 * 1024)
+      rd_scatter_kernel<false><<<dim3((n + 127) / 128, na, zc), 128, 0, s>>>(
+          d_sino + (size_t)z0 * per_sino, accf, accT, lines, flags, (const RdAngle *)p.d_angles,
+          (const float *)p.d_aux, n, p.nh, na, smax + z0);
+    else
+      rd_scatter_kernel<true><<<dim3((5 * n + 127) / 128, na, zc), 128, 0, s>>>(
+          d_sino + (size_t)z0 * per_sino, accf, accT, lines, flags, (const RdAngle *)p.d_angles,
+          (const float *)p.d_aux, n, p.nh, na, smax + z0);
     rd_finalize_kernel<<<dim3((n + 31) / 32, (n + 31) / 32, zc), dim3(32, 8), 0, s>>>(
         accf, accT, lines, flags, d_img, n, z0, na, smax + z0, ep);
   }

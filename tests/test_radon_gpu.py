@@ -103,6 +103,26 @@ def test_deterministic_and_batched(cuda, kind):
     assert np.array_equal(tp.At(yd).cpu().numpy(), g1)
 
 
+def test_rd_adjoint_thread_layouts_agree(cuda):
+    """The rd adjoint runs one thread per bin when bins x angles x slices reach
+    148 x 1024, else one thread per sub-ray; both make the same fixed-point
+    credits, so the results are the same bits.  Here the 3-slice batch
+    (256 x 200 x 3 = 153,600) takes the first layout and each slice alone
+    (51,200) the second; non-finite values and the axis angles' row and column
+    sums (made by a bin's first thread only) are included."""
+    n, na, nz = 256, 200, 3
+    assert n * na * nz >= 148 * 1024 > n * na
+    rng = np.random.default_rng(17)
+    y = rng.standard_normal((nz, na, n)).astype(np.float32)
+    y[1, 7, 100] = np.inf
+    y[2, 150, 31] = np.nan
+    deg = np.linspace(0, 180, na, endpoint=False)  # includes 0 and 90 degrees
+    tp = _proj("rd", n, deg)
+    batched = tp.At(y)
+    for z in range(nz):
+        assert np.array_equal(tp.At(y[z]).view(np.uint32), batched[z].view(np.uint32)), z
+
+
 @pytest.mark.parametrize("kind", KINDS)
 def test_dropin_entry_point_accumulates(cuda, radon_golden, kind):
     """tomo_radon_<kind> has the reference C signature and accumulates like it."""
