@@ -13,7 +13,8 @@
 // column in [1, n-1]; it stops after the first step with alpha > 1.
 //
 // Both directions run the same walks (rd_walk_loop), one thread per (bin, angle,
-// slice) replaying its bin's five sub-rays:
+// slice) replaying its bin's five sub-rays (the adjoint, on grids too small to
+// fill the GPU, one thread per sub-ray):
 //   forward  gathers 0.2 l x[pixel] into the bin, in walk order;
 //   adjoint  scatters 0.2 l y[bin] into a 64-bit fixed-point image with
 //            integer reductions (order-independent sums, so deterministic, of
@@ -282,16 +283,22 @@ __global__ void rd_frame_kernel(const float *__restrict__ in, float *__restrict_
 }
 
 // Forward over slices z0 + blockIdx.z; Q and QT hold the chunk's slices
-// framed (rd_frame_kernel).  A block is 128 bins of kFwdAngles consecutive
+// framed (rd_frame_kernel).  A block is kBins bins of kFwdAngles consecutive
 // angles (threadIdx.y): the walks of neighbouring angles cover nearly the same
-// pixels at nearly the same time, so its warps share L1 lines.
+// pixels at nearly the same time, so its warps share L1 lines.  kBins = 128,
+// or 32 for grids of at most a few blocks per SM, where 512-thread blocks
+// leave some SMs with one more block than others (at 256 x 256, 304 angles:
+// 152 blocks on 148 SMs, two resident per SM).  A row of the sinogram has
+// ceil(n / 128) * 4 warps in both layouts (dead lanes included), and warp
+// b / 32 of row (z, v) writes residual slot (z na + v) * that + b / 32.
 constexpr int kFwdAngles = 4;
 
-__global__ void __launch_bounds__(128 * kFwdAngles, 8 / kFwdAngles) rd_forward_kernel(
+template <int kBins>
+__global__ void __launch_bounds__(kBins * kFwdAngles, 1024 / (kBins * kFwdAngles)) rd_forward_kernel(
     const float *__restrict__ img, const float *__restrict__ Q, const float *__restrict__ QT,
     float *__restrict__ sino, const RdAngle *__restrict__ tab, const float *__restrict__ toff, int n, int nh, int na,
     int z0, FwdEpi ep) {
-  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  const int b = blockIdx.x * kBins + threadIdx.x;
   const int v = blockIdx.y * kFwdAngles + threadIdx.y;
   if (v >= na) return;  // whole warps
   const size_t z = (size_t)z0 + blockIdx.z;
@@ -326,7 +333,7 @@ __global__ void __launch_bounds__(128 * kFwdAngles, 8 / kFwdAngles) rd_forward_k
   const size_t e = (z * na + v) * (size_t)n + (live ? b : 0);
   double r2 = 0.0;
   if (live) sino[e] = fwd_apply(ep, acc, e, r2);
-  fwd_resid_commit(ep, r2, ((z * na + v) * gridDim.x + blockIdx.x) * (blockDim.x / 32) + threadIdx.x / 32);
+  fwd_resid_commit(ep, r2, (z * na + v) * (gridDim.x * (kBins / 32)) + b / 32);
 }
 
 // Flag bytes of non-finite credits (nonfinite_flag: 1 +inf, 2 -inf, 4 NaN),
@@ -516,8 +523,14 @@ int rd_forward(Plan &p, const float *d_img, float *d_sino, cudaStream_t s, const
     const int zc = std::min(chunk, nz - z0);
     rd_frame_kernel<<<dim3((m + 31) / 32, (m + 31) / 32, zc), dim3(32, 8), 0, s>>>(d_img + (size_t)z0 * n * n, Q,
                                                                                      QT, n);
-    rd_forward_kernel<<<dim3((n + 127) / 128, (na + kFwdAngles - 1) / kFwdAngles, zc), dim3(128, kFwdAngles), 0, s>>>(
-        d_img, Q, QT, d_sino, (const RdAngle *)p.d_angles, (const float *)p.d_aux, n, p.nh, na, z0, ep);
+    const int rows = (na + kFwdAngles - 1) / kFwdAngles, w128 = (n + 127) / 128;
+    // 128-bin blocks once there are 8 or more per SM, else 32-bin ones
+    if ((size_t)w128 * rows * zc >= (size_t)148 * 8)
+      rd_forward_kernel<128><<<dim3(w128, rows, zc), dim3(128, kFwdAngles), 0, s>>>(
+          d_img, Q, QT, d_sino, (const RdAngle *)p.d_angles, (const float *)p.d_aux, n, p.nh, na, z0, ep);
+    else
+      rd_forward_kernel<32><<<dim3(4 * w128, rows, zc), dim3(32, kFwdAngles), 0, s>>>(
+          d_img, Q, QT, d_sino, (const RdAngle *)p.d_angles, (const float *)p.d_aux, n, p.nh, na, z0, ep);
   }
   TOMO_CUDA(cudaGetLastError());
   return TOMO_OK;

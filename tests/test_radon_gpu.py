@@ -103,24 +103,32 @@ def test_deterministic_and_batched(cuda, kind):
     assert np.array_equal(tp.At(yd).cpu().numpy(), g1)
 
 
-def test_rd_adjoint_thread_layouts_agree(cuda):
-    """The rd adjoint runs one thread per bin when bins x angles x slices reach
-    148 x 1024, else one thread per sub-ray; both make the same fixed-point
-    credits, so the results are the same bits.  Here the 3-slice batch
-    (256 x 200 x 3 = 153,600) takes the first layout and each slice alone
-    (51,200) the second; non-finite values and the axis angles' row and column
-    sums (made by a bin's first thread only) are included."""
-    n, na, nz = 256, 200, 3
+def test_rd_thread_layouts_agree(cuda):
+    """Both rd kernels pick their thread layout by grid size, and the layouts
+    make the same arithmetic in the same order, so the results are the same
+    bits.  The forward runs blocks of 128 bins x 4 angles once there are 8 or
+    more such blocks per SM (148 SMs), else blocks of 32 bins x 4 angles; the
+    adjoint runs one thread per bin when bins x angles x slices reach
+    148 x 1024, else one thread per sub-ray.  Here the 12-slice batch of
+    256 x 256 at 200 angles (1200 blocks; 614,400 threads) takes the first
+    layout of each and a slice alone (100 blocks; 51,200 threads) the second.
+    Non-finite values and the axis angles' row and column sums (made by a
+    bin's first thread only in the adjoint) are included."""
+    n, na, nz = 256, 200, 12
+    assert 2 * (na // 4) * nz >= 148 * 8 > 2 * (na // 4)
     assert n * na * nz >= 148 * 1024 > n * na
     rng = np.random.default_rng(17)
+    x = rng.standard_normal((nz, n, n)).astype(np.float32)
     y = rng.standard_normal((nz, na, n)).astype(np.float32)
     y[1, 7, 100] = np.inf
     y[2, 150, 31] = np.nan
+    x[3, 60, 70] = -np.inf
     deg = np.linspace(0, 180, na, endpoint=False)  # includes 0 and 90 degrees
     tp = _proj("rd", n, deg)
-    batched = tp.At(y)
+    fwd, adj = tp.A(x), tp.At(y)
     for z in range(nz):
-        assert np.array_equal(tp.At(y[z]).view(np.uint32), batched[z].view(np.uint32)), z
+        assert np.array_equal(tp.A(x[z]).view(np.uint32), fwd[z].view(np.uint32)), z
+        assert np.array_equal(tp.At(y[z]).view(np.uint32), adj[z].view(np.uint32)), z
 
 
 @pytest.mark.parametrize("kind", KINDS)
